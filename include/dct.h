@@ -1,0 +1,191 @@
+/*
+ * dct.h -- C ABI of libdct, the B200 (sm_100a) sparse direct solver and DC
+ * forward/adjoint kernels behind simpeg_dc_torch_b200.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (DCT_OK = 0).  On failure
+ *     dct_last_error() returns a message for the calling thread.  No C++
+ *     exception and no device trap crosses this boundary.
+ *   - Pointers named d_* are device pointers on the plan's device; all other
+ *     pointers are host pointers.  `stream` is a cudaStream_t (NULL = legacy
+ *     default stream); work is enqueued asynchronously on it.
+ *   - Dense right-hand sides are row-major (n, k) per system, k contiguous,
+ *     the layout of a torch (n, k) tensor; batched ones are (nbatch, n, k).
+ *   - "Permuted" buffers hold rows in the solver's elimination order
+ *     (row i of the permuted buffer is row perm[i] of the user's ordering).
+ *
+ * Each declaration names the reference interface it replaces
+ * (eacuellarq/SimPEG_DC_Torch, dctorch 0.2.0, path:line).
+ */
+#ifndef DCT_H
+#define DCT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { DCT_F64 = 0, DCT_F32 = 1 };
+
+enum {
+  DCT_OK = 0,
+  DCT_ERR_ARG = 1,              /* invalid argument */
+  DCT_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+  DCT_ERR_OOM = 3,              /* device allocation failed */
+  DCT_ERR_ZERO_PIVOT = 4,       /* non-positive pivot: matrix not SPD */
+  DCT_ERR_IR_NOT_CONVERGED = 5, /* refinement residual above tolerance */
+  DCT_ERR_BAD_PATTERN = 6,      /* pattern rejected by the analysis */
+  DCT_ERR_NOT_FACTORED = 7,     /* solve before factorize */
+  DCT_ERR_NO_DEVICE = 8         /* no usable CUDA device */
+};
+
+typedef struct dct_symbolic dct_symbolic;
+typedef struct dct_plan dct_plan;
+
+typedef struct {
+  int64_t n;             /* unknowns */
+  int64_t nnz_in;        /* entries of the input pattern */
+  int64_t nsuper;        /* supernodes (dense fronts) */
+  int64_t nlevels;       /* levels of the assembly tree */
+  int64_t max_front;     /* largest front order */
+  int64_t max_ns;        /* largest supernode (pivot columns) */
+  int64_t nnz_L;         /* stored factor entries, explicit zeros included */
+  int64_t front_total;   /* front storage per system, in elements */
+  double flops_factor;   /* dense flops of one numeric factorization */
+} dct_symbolic_info;
+
+int dct_version(void);
+const char* dct_last_error(void);
+
+/* ---- symbolic analysis (host only; no GPU needed) ------------------------
+ * Nested-dissection ordering, assembly tree and front maps of a structurally
+ * symmetric CSR pattern (int32 crow[n+1], col[nnz]).  coords (n x ndim
+ * int32, may be NULL) are grid coordinates for geometric bisection.
+ * Replaces the reordering + symbolic phase of DirectSolver(...).plan()
+ * (dctorch/solver.py:103-109, 204-207). */
+int dct_symbolic_create(int32_t n, const int32_t* crow, const int32_t* col,
+                        const int32_t* coords, int32_t ndim, int32_t leaf_size,
+                        dct_symbolic** out);
+void dct_symbolic_destroy(dct_symbolic* sym);
+int dct_symbolic_get_info(const dct_symbolic* sym, dct_symbolic_info* out);
+/* Copies a named int32/int64 array of the analysis (perm, iperm, sn_first,
+ * sn_parent, sn_level, front_n, front_off, rows_ptr, rows, child_ptr, child,
+ * rel_ptr, rel, amap_ptr, amap_e, amap_pos) into dst.  With dst NULL only
+ * *size_bytes is set. */
+int dct_symbolic_get_array(const dct_symbolic* sym, const char* name,
+                           void* dst, int64_t capacity_bytes,
+                           int64_t* size_bytes);
+
+/* Host-side copy of the launch schedule a plan of this dtype would run
+ * (which: 0 factorization, 1 forward, 2 backward substitution), for
+ * inspection and CPU-side replay in tests.  tasks: 4 int32 per task
+ * (supernode, panel, t0, t1); launches: 5 int64 per launch (kind, level,
+ * first task, task count, arg).  With null outputs only the counts are set. */
+int dct_symbolic_get_schedule(const dct_symbolic* sym, int32_t dtype,
+                              int32_t which, int32_t* tasks, int64_t* ntasks,
+                              int64_t* launches, int64_t* nlaunches);
+
+/* ---- numeric plan: nbatch systems on one pattern, on one device -----------
+ * dtype DCT_F64: plain float64 factor and solve.
+ * dtype DCT_F32: float32 factor and solve, with iterative refinement whose
+ *                residual b - A x is formed in float64.
+ * Replaces CuDSSSolver.__init__ (dctorch/solver.py:88-114) and
+ * CuDSSBatchSolver.__init__ (dctorch/solver.py:187-213). */
+int dct_plan_create(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
+                    int32_t dtype, int32_t device, dct_plan** out);
+void dct_plan_destroy(dct_plan* plan);
+int dct_plan_set_refinement(dct_plan* plan, int32_t iterations);
+/* device pointer to the plan's iperm (int32, n): user row -> permuted row */
+int dct_plan_iperm(const dct_plan* plan, const int32_t** d_iperm);
+/* bumped by every factorization (dctorch/solver.py:211-213, 221) */
+int64_t dct_plan_stamp(const dct_plan* plan);
+
+/* Numeric factorization of every system from its CSR values.
+ * d_vals: nbatch rows of nnz values, row b at d_vals + b*vals_batch_stride,
+ * float64 or float32 (vals_dtype).  Replaces CuDSSSolver.factorize
+ * (dctorch/solver.py:116-120) and CuDSSBatchSolver.factorize (215-221). */
+int dct_factorize(dct_plan* plan, const void* d_vals, int32_t vals_dtype,
+                  int64_t vals_batch_stride, void* stream);
+
+/* Solve every system for k <= max_rhs right-hand sides in the user's row
+ * order.  d_b: (n, k) shared by all systems (b_batched = 0) or
+ * (nbatch, n, k); d_x: (nbatch, n, k).  io_dtype gives the type of both.
+ * Replaces CuDSSSolver.solve (dctorch/solver.py:122-135) and
+ * CuDSSBatchSolver.solve (dctorch/solver.py:223-230). */
+int dct_solve(dct_plan* plan, const void* d_b, int32_t io_dtype,
+              int32_t b_batched, int32_t k, void* d_x, void* stream);
+
+/* The same solve on float64 buffers already in permuted order:
+ * d_bp (n, k) shared or (nbatch, n, k); d_xp (nbatch, n, k).  d_bp may alias
+ * d_xp only when batched.  Used by the fused engine paths. */
+int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
+                       int32_t k, double* d_xp, void* stream);
+
+/* Reads the device status words (synchronises the stream): the first error
+ * code raised by a kernel since the last call, the supernode where it was
+ * raised (or -1) and the last refinement residual ratio max|b-Ax|/max|b|. */
+int dct_check_status(dct_plan* plan, void* stream, int32_t* code,
+                     int32_t* where, double* residual);
+
+/* ---- fused engine kernels (stateless; float64) ---------------------------- */
+
+/* sigma = exp(-m) (nC) and vals = L sigma for a CSR L with nrows rows
+ * (int64 row pointers).  Replaces the value build of TorchDC2D.dpred /
+ * TorchDC3D.dpred: torch.sparse.mm(Lstack, exp(-m)) (dctorch/
+ * simulation2d.py:391-392, simulation3d.py:203-204). */
+int dct_sigma_values(int64_t nrows, const int64_t* d_L_ptr,
+                     const int32_t* d_L_col, const double* d_L_val,
+                     int64_t nC, const double* d_m, double* d_sigma,
+                     double* d_vals, void* stream);
+
+/* gm = -sigma * (Lt gv): the vjp of vals = L exp(-m), with Lt the CSR of L^T
+ * (nC rows).  Replaces the autograd backward of torch.sparse.mm(Lstack, .)
+ * and of exp (dctorch/simulation2d.py:391-392; simulation3d.py:25-41). */
+int dct_values_vjp(int64_t nC, const int64_t* d_Lt_ptr, const int32_t* d_Lt_col,
+                   const double* d_Lt_val, const double* d_sigma,
+                   const double* d_gv, double* d_gm, void* stream);
+
+/* dst(n, k) = 0, then dst[row[p]*k + src[p]] = sum over q in [ptr[p],
+ * ptr[p+1]) of coef[q] * (d_g ? g[datum[q]] : 1).  Builds the permuted source
+ * right-hand side (q, dctorch/simulation2d.py:231-234, 325-328) and the
+ * adjoint right-hand side Pd^T G (the vjp of the projection/gather,
+ * dctorch/simulation2d.py:395). */
+int dct_scatter_rhs(int64_t n, int32_t k, int64_t npairs, const int64_t* d_ptr,
+                    const int32_t* d_row, const int32_t* d_src,
+                    const int32_t* d_datum, const double* d_coef,
+                    const double* d_g, double* d_dst, void* stream);
+
+/* d[i] = sum_b w[b] sum_{j in Pd row i} Pd[i,j] X[b, iperm[j], sidx[i]]:
+ * wavenumber quadrature sum + receiver projection + per-datum source
+ * gather, fused (dctorch/simulation2d.py:394-395; simulation3d.py:206).
+ * X permuted (nbatch, n, k); d_w may be NULL (all ones). */
+int dct_project_data(int32_t nbatch, int64_t n, int32_t k, int64_t nD,
+                     const int32_t* d_Pd_ptr, const int32_t* d_Pd_col,
+                     const double* d_Pd_val, const int32_t* d_sidx,
+                     const int32_t* d_iperm, const double* d_w,
+                     const double* d_X, double* d_out, void* stream);
+
+/* gv[b, e] = -scale[b] * sum_r Y[b, iperm[row_e], r] X[b, iperm[col_e], r]:
+ * the value gradient of the batched solve on the pattern
+ * (dctorch/solver.py:268-276 with the quadrature weight of
+ * simulation2d.py:394 folded in).  X, Y permuted (nbatch, n, k);
+ * d_scale may be NULL (all ones). */
+int dct_gather_contract(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
+                        const int32_t* d_row, const int32_t* d_col,
+                        const int32_t* d_iperm, const double* d_scale,
+                        const double* d_Y, const double* d_X, double* d_gv,
+                        void* stream);
+
+/* Same contraction in the user's row order and dtype, for the solver-level
+ * autograd op: gv[b,e] = -sum_r Y[b,row_e,r] X[b,col_e,r]
+ * (dctorch/solver.py:160-170, 268-276). */
+int dct_gather_contract_plain(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
+                              const int32_t* d_row, const int32_t* d_col,
+                              int32_t dtype, const void* d_Y, const void* d_X,
+                              void* d_gv, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCT_H */

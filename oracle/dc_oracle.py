@@ -1,0 +1,188 @@
+"""CPU oracle (TEST INFRASTRUCTURE ONLY) for dctorch's forward + adjoint path.
+
+A float64 numpy/scipy restatement of what the reference computes at run
+time, given the build-time operators.  It is used by the tests as the checker
+and by bench.py as the timed CPU baseline; the product never calls it.
+
+Pinned: `tests/golden/*.npz` hold outputs of the reference itself (its
+`SciPySolver`/`SciPyBatchSolver` SuperLU path and its `TorchDC2D`/`TorchDC3D`
+runtime, driven with the same operators); `tests/test_oracle.py` checks this
+module against them.
+
+Operators (names as in the reference engines):
+  Lstack  : CSR (nky*nnzA, nC), values of A_k = rows k*nnzA .. (k+1)*nnzA
+  crow,col: CSR pattern of A (nN+1,), (nnzA,)
+  wq      : (nky,) quadrature weights            (2.5-D only)
+  Q       : (nN, nS) dense sources
+  Pd      : CSR (nD, nN) receiver projection;  sidx (nD,) source of datum
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+
+# ------------------------------------------------------------- solver level
+class SuperLUBatch:
+    """SuperLU factorizations of nbatch systems on one pattern
+    (dctorch/solver.py:314-374, SciPySolver / SciPyBatchSolver)."""
+
+    def __init__(self, crow, col, n):
+        self.crow = np.asarray(crow)
+        self.col = np.asarray(col)
+        self.n = int(n)
+        self.lu = []
+
+    def factorize(self, vals):
+        vals = np.atleast_2d(np.asarray(vals, float))
+        self.lu = [spla.splu(sp.csr_matrix((v, self.col, self.crow),
+                                           shape=(self.n, self.n)).tocsc())
+                   for v in vals]
+
+    def solve(self, B):
+        """B: (n, k) shared, or (nbatch, n, k); returns (nbatch, n, k)."""
+        B = np.asarray(B, float)
+        if B.ndim == 2:
+            return np.stack([lu.solve(B) for lu in self.lu])
+        return np.stack([lu.solve(B[i]) for i, lu in enumerate(self.lu)])
+
+
+def row_of(crow):
+    return np.repeat(np.arange(len(crow) - 1), np.diff(crow))
+
+
+def sparse_solve_vjp(crow, col, vals, b, gx):
+    """x = A^{-1} b and the vector-Jacobian products of a loss with dL/dx = gx
+    (dctorch/solver.py:141-173 and 261-281):
+        adj = A^{-1} gx;  dL/dvals[e] = -sum_s adj[row_e, s] x[col_e, s];
+        dL/db = adj  (summed over the batch when b is shared).
+    vals: (nnz,) or (nb, nnz); b: (n,k) or (nb,n,k); gx like x.
+    """
+    vals = np.asarray(vals, float)
+    single = vals.ndim == 1
+    V = vals[None] if single else vals
+    n = len(crow) - 1
+    slv = SuperLUBatch(crow, col, n)
+    slv.factorize(V)
+    b = np.asarray(b, float)
+    b2 = b.reshape(n, -1) if (single and b.ndim <= 2) else b
+    x = slv.solve(b2 if b2.ndim == 2 else b2)
+    gx = np.asarray(gx, float)
+    G = gx.reshape(x.shape)
+    adj = slv.solve(G) if G.ndim == 3 else slv.solve(G)
+    r = row_of(crow)
+    gvals = -np.einsum("bes,bes->be", adj[:, r, :], x[:, col, :])
+    shared = b.ndim == 2 or single
+    gb = adj.sum(0) if (shared and not single) else adj
+    if single:
+        return x[0].reshape(b.shape), gvals[0], adj[0].reshape(b.shape)
+    return x, gvals, gb
+
+
+# ---------------------------------------------------------- engine level
+def sigma_of(m):
+    return np.exp(-np.asarray(m, float))
+
+
+def vals_2d(Lstack, m, nky):
+    """VALS = (Lstack @ exp(-m)).view(nky, nnzA)  (simulation2d.py:391-392)."""
+    v = Lstack @ sigma_of(m)
+    return v.reshape(nky, -1)
+
+
+def dpred_2d(op, m, return_fields=False):
+    """Predicted data (simulation2d.py:378-396): Ubar = sum_k wq_k U_k,
+    d = (Pd Ubar)[i, sidx[i]]."""
+    nky = len(op["wq"])
+    VALS = vals_2d(op["Lstack"], m, nky)
+    slv = SuperLUBatch(op["crow"], op["col"], op["nN"])
+    slv.factorize(VALS)
+    U = slv.solve(op["Q"])
+    Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
+    PU = op["Pd"] @ Ubar
+    d = PU[np.arange(PU.shape[0]), op["sidx"]]
+    if return_fields:
+        return d, VALS, slv, U
+    return d
+
+
+def _adjoint_2d(op, m, g_data):
+    """dL/dm for dL/dd = g_data through the 2.5-D chain (the autograd path of
+    simulation2d.py:378-396 with solver.py:261-281 and the Lstack vjp)."""
+    nky = len(op["wq"])
+    d, VALS, slv, U = dpred_2d(op, m, return_fields=True)
+    nS = op["Q"].shape[1]
+    nN = op["nN"]
+    # dL/dUbar[:, s] = Pd^T (g restricted to source s)
+    G = np.zeros((op["Pd"].shape[0], nS))
+    G[np.arange(G.shape[0]), op["sidx"]] = g_data
+    GU = op["Pd"].T @ G                         # (nN, nS)
+    Y = slv.solve(GU)                           # A_k^{-1} Pd^T G (unweighted)
+    r = row_of(op["crow"])
+    gv = np.empty((nky, len(op["col"])))
+    for k in range(nky):
+        gv[k] = -op["wq"][k] * np.einsum("es,es->e", Y[k][r], U[k][op["col"]])
+    gsig = op["Lstack"].T @ gv.reshape(-1)
+    return d, -sigma_of(m) * gsig
+
+
+def misfit_2d(op, m, dobs, w):
+    """phi = sum (w (d - dobs))^2 (simulation2d.py:531-534)."""
+    d = dpred_2d(op, m)
+    r = w * (d - dobs)
+    return float((r ** 2).sum())
+
+
+def misfit_grad_2d(op, m, dobs, w):
+    d = dpred_2d(op, m)
+    r = w * (d - dobs)
+    _, g = _adjoint_2d(op, m, 2.0 * w * r)
+    return float((r ** 2).sum()), g
+
+
+def jtvec_2d(op, m, v):
+    """J^T v (simulation2d.py:398-437)."""
+    return _adjoint_2d(op, m, np.asarray(v, float))[1]
+
+
+# ------------------------------------------------------------------- 3-D
+def dpred_3d(op, m, return_fields=False):
+    """simulation3d.py:197-207: VALS = L3 exp(-m); U = A^{-1} q; d = (Pd U)[i, sidx]."""
+    vals = op["L3"] @ sigma_of(m)
+    slv = SuperLUBatch(op["crow"], op["col"], op["nN"])
+    slv.factorize(vals[None])
+    U = slv.solve(op["Q"])[0]
+    PU = op["Pd"] @ U
+    d = PU[np.arange(PU.shape[0]), op["sidx"]]
+    if return_fields:
+        return d, slv, U
+    return d
+
+
+def _adjoint_3d(op, m, g_data):
+    d, slv, U = dpred_3d(op, m, return_fields=True)
+    G = np.zeros((op["Pd"].shape[0], op["Q"].shape[1]))
+    G[np.arange(G.shape[0]), op["sidx"]] = g_data
+    Y = slv.solve(op["Pd"].T @ G)[0]
+    r = row_of(op["crow"])
+    gv = -np.einsum("es,es->e", Y[r], U[op["col"]])
+    return d, -sigma_of(m) * (op["L3"].T @ gv)
+
+
+def misfit_grad_3d(op, m, dobs, w):
+    d = dpred_3d(op, m)
+    r = w * (d - dobs)
+    _, g = _adjoint_3d(op, m, 2.0 * w * r)
+    return float((r ** 2).sum()), g
+
+
+def jtvec_3d(op, m, v):
+    """simulation3d.py:209-222."""
+    return _adjoint_3d(op, m, np.asarray(v, float))[1]
+
+
+def rel(a, b):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

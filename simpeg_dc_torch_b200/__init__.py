@@ -1,0 +1,23 @@
+"""simpeg_dc_torch_b200 -- the dctorch DC forward + adjoint hot path on B200.
+
+A from-scratch sm_100a implementation (sparse supernodal Cholesky, multi-RHS
+substitution, fused assembly / projection / adjoint kernels) behind the
+reference's solver and engine interfaces:
+
+    make_solver, make_batch_solver, DCTSolver, DCTBatchSolver,
+    sparse_solve, sparse_solve_batch, sparse_solve_batch_prefactored,
+    TorchDC2D, TorchDC3D
+
+Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
+discretize / SimPEG objects, which may be passed instead.
+"""
+__version__ = "0.1.0"
+
+from .mesh import TensorMesh  # noqa: F401
+from .survey import (DipoleReceiver, DipoleSource, PoleReceiver,  # noqa: F401
+                     PoleSource, Survey)
+from .solver import (CuDSSBatchSolver, CuDSSSolver, DCTBatchSolver,  # noqa: F401
+                     DCTSolver, make_batch_solver, make_solver, sparse_solve,
+                     sparse_solve_batch, sparse_solve_batch_prefactored)
+from .simulation2d import TorchDC2D  # noqa: F401
+from .simulation3d import TorchDC3D  # noqa: F401

@@ -1,0 +1,211 @@
+"""The fused forward + adjoint path shared by the 2.5-D and 3-D engines.
+
+One call of `forward` runs, on the engine's CUDA stream,
+
+    sigma = exp(-m);  VALS = L sigma                  (dct_sigma_values)
+    factor every system                               (dct_factorize)
+    U = A^{-1} Q for all sources, all systems         (dct_scatter_rhs + dct_solve_permuted)
+    d_i = sum_k w_k (Pd U_k)[i, sidx_i]               (dct_project_data)
+
+and `adjoint(gd)` the reverse pass for dL/dd = gd on the same factors,
+
+    R = Pd^T G (scattered into source columns)        (dct_scatter_rhs)
+    Y = A^{-1} R                                      (dct_solve_permuted)
+    gv[k, e] = -w_k sum_s Y_k[row_e, s] U_k[col_e, s] (dct_gather_contract)
+    dL/dm = -sigma * (L^T gv)                         (dct_values_vjp)
+
+which is the chain the reference builds from torch ops and cuDSS calls
+(dctorch/simulation2d.py:378-396 with solver.py:236-281; simulation3d.py:
+197-207).  Fields stay in the solver's permuted row order on the device.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from . import _native as nat
+from .solver import DCTBatchSolver, _stream_ptr
+
+
+def _csr64(M: sp.csr_matrix, device):
+    M = sp.csr_matrix(M)
+    M.sum_duplicates()
+    M.sort_indices()
+    return (torch.as_tensor(M.indptr.astype(np.int64), device=device),
+            torch.as_tensor(M.indices.astype(np.int32), device=device),
+            torch.as_tensor(M.data.astype(np.float64), device=device))
+
+
+class FusedPath:
+    """Device operators + solver for one mesh/survey.
+
+    L      : (nbatch*nnzA, nC) assembly map (scipy CSR), system k in rows
+             k*nnzA .. (k+1)*nnzA
+    w      : per-system weights of the data sum (None: all ones)
+    Q      : (nN, nS) scipy sparse sources;  Pd (nD, nN) CSR; sidx (nD,)
+    """
+
+    def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
+                 coords=None, refine=None, n_rhs=None):
+        self.device = device
+        nN = crow.size - 1
+        self.nN, self.nnzA = nN, col.size
+        self.nbatch = L.shape[0] // self.nnzA
+        self.nC = L.shape[1]
+        self.nS = Q.shape[1]
+        self.nD = Pd.shape[0]
+        dt = torch.float64 if precision == "fp64" else torch.float32
+        self.width = int(n_rhs or self.nS)
+        self.solver = DCTBatchSolver(crow, col, nN, self.width, self.nbatch,
+                                     device=device, dtype=dt, coords=coords,
+                                     refine=refine)
+        plan = self.solver.plan
+        self._plan = plan
+        self._iperm_ptr = plan.d_iperm
+        perm = self.solver._sym.array("perm")
+        iperm = np.empty_like(perm)
+        iperm[perm] = np.arange(perm.size, dtype=perm.dtype)
+        self.iperm_host = iperm
+        self.L_ptr, self.L_col, self.L_val = _csr64(L, device)
+        self.Lt_ptr, self.Lt_col, self.Lt_val = _csr64(sp.csr_matrix(L.T), device)
+        self.w = None if w is None else torch.as_tensor(
+            np.asarray(w, float), device=device)
+        self.row_e = self.solver.row
+        self.col_e = self.solver.col
+        # sources: one pair per nonzero (node, source)
+        Qc = sp.coo_matrix(Q)
+        self._q = self._pairs(iperm[Qc.row], Qc.col,
+                              [[(0, v)] for v in Qc.data])
+        # receivers: CSR of Pd and the adjoint pairs (node, source) <- data
+        Pd = sp.csr_matrix(Pd)
+        Pd.sort_indices()
+        self.Pd_ptr = torch.as_tensor(Pd.indptr.astype(np.int32), device=device)
+        self.Pd_col = torch.as_tensor(Pd.indices.astype(np.int32), device=device)
+        self.Pd_val = torch.as_tensor(Pd.data.astype(np.float64), device=device)
+        self.sidx = np.asarray(sidx, dtype=np.int64)
+        self.sidx_d = torch.as_tensor(self.sidx.astype(np.int32), device=device)
+        groups = {}
+        Pc = Pd.tocoo()
+        for i, j, v in zip(Pc.row, Pc.col, Pc.data):
+            key = (int(iperm[j]), int(self.sidx[i]))
+            groups.setdefault(key, []).append((int(i), float(v)))
+        keys = sorted(groups)
+        self._adj = self._pairs(np.array([k[0] for k in keys], dtype=np.int64),
+                                np.array([k[1] for k in keys], dtype=np.int64),
+                                [groups[k] for k in keys])
+
+    def _pairs(self, rows, srcs, lists):
+        ptr = np.zeros(len(lists) + 1, dtype=np.int64)
+        ptr[1:] = np.cumsum([len(x) for x in lists])
+        datum = np.array([d for x in lists for d, _ in x], dtype=np.int32)
+        coef = np.array([c for x in lists for _, c in x], dtype=np.float64)
+        dev = self.device
+        return dict(n=len(lists),
+                    ptr=torch.as_tensor(ptr, device=dev),
+                    row=torch.as_tensor(np.asarray(rows, np.int32), device=dev),
+                    src=torch.as_tensor(np.asarray(srcs, np.int32), device=dev),
+                    datum=torch.as_tensor(datum, device=dev),
+                    coef=torch.as_tensor(coef, device=dev))
+
+    # ------------------------------------------------------------ kernels
+    def _st(self):
+        return _stream_ptr(self.device)
+
+    def values(self, m_full):
+        """sigma, VALS (nbatch, nnzA) for the full-mesh log-resistivity."""
+        m = m_full.detach().to(self.device, torch.float64).contiguous()
+        sigma = torch.empty(self.nC, dtype=torch.float64, device=self.device)
+        vals = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
+                           device=self.device)
+        nat.check(nat.lib().dct_sigma_values(
+            vals.numel(), self.L_ptr.data_ptr(), self.L_col.data_ptr(),
+            self.L_val.data_ptr(), self.nC, m.data_ptr(), sigma.data_ptr(),
+            vals.data_ptr(), self._st()), "dct_sigma_values")
+        return sigma, vals.view(self.nbatch, self.nnzA)
+
+    def factorize(self, vals):
+        self.solver.factorize(vals)
+
+    def _scatter(self, pairs, g, k):
+        dst = torch.empty((self.nN, k), dtype=torch.float64, device=self.device)
+        nat.check(nat.lib().dct_scatter_rhs(
+            self.nN, k, pairs["n"], pairs["ptr"].data_ptr(),
+            pairs["row"].data_ptr(), pairs["src"].data_ptr(),
+            pairs["datum"].data_ptr(), pairs["coef"].data_ptr(),
+            None if g is None else g.data_ptr(), dst.data_ptr(), self._st()),
+            "dct_scatter_rhs")
+        return dst
+
+    def _solve_perm(self, rhs_shared, k):
+        x = torch.empty((self.nbatch, self.nN, k), dtype=torch.float64,
+                        device=self.device)
+        self._plan.solve_permuted(rhs_shared.data_ptr(), 0, k, x.data_ptr(),
+                                  self._st())
+        return x
+
+    def fields(self):
+        """U = A^{-1} Q, permuted (nbatch, nN, nS)."""
+        return self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
+
+    def project(self, U):
+        d = torch.empty(self.nD, dtype=torch.float64, device=self.device)
+        nat.check(nat.lib().dct_project_data(
+            self.nbatch, self.nN, U.shape[-1], self.nD, self.Pd_ptr.data_ptr(),
+            self.Pd_col.data_ptr(), self.Pd_val.data_ptr(),
+            self.sidx_d.data_ptr(), self._iperm_ptr,
+            None if self.w is None else self.w.data_ptr(), U.data_ptr(),
+            d.data_ptr(), self._st()), "dct_project_data")
+        return d
+
+    def forward(self, m_full):
+        """(d, sigma, U, stamp): data, conductivity, permuted fields and the
+        solver stamp of the factorization they were computed with."""
+        sigma, vals = self.values(m_full)
+        self.factorize(vals)
+        U = self.fields()
+        d = self.project(U)
+        return d, sigma, U, self.solver.stamp
+
+    def ensure_factors(self, m_full, stamp):
+        """Refactorize at m_full if another call replaced the factors."""
+        if self.solver.stamp != stamp:
+            self.factorize(self.values(m_full)[1])
+        return self.solver.stamp
+
+    def adjoint(self, gd, U, sigma):
+        """dL/dm_full for dL/dd = gd on the current factorization."""
+        g = gd.detach().to(self.device, torch.float64).contiguous()
+        R = self._scatter(self._adj, g, self.nS)
+        Y = self._solve_perm(R, self.nS)
+        gv = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
+                         device=self.device)
+        nat.check(nat.lib().dct_gather_contract(
+            self.nbatch, self.nN, self.nnzA, self.nS, self.row_e.data_ptr(),
+            self.col_e.data_ptr(), self._iperm_ptr,
+            None if self.w is None else self.w.data_ptr(), Y.data_ptr(),
+            U.data_ptr(), gv.data_ptr(), self._st()), "dct_gather_contract")
+        gm = torch.empty(self.nC, dtype=torch.float64, device=self.device)
+        nat.check(nat.lib().dct_values_vjp(
+            self.nC, self.Lt_ptr.data_ptr(), self.Lt_col.data_ptr(),
+            self.Lt_val.data_ptr(), sigma.data_ptr(), gv.data_ptr(),
+            gm.data_ptr(), self._st()), "dct_values_vjp")
+        return gm
+
+
+class FusedDpred(torch.autograd.Function):
+    """d = dpred(m_full) with the hand-written adjoint as its backward."""
+
+    @staticmethod
+    def forward(ctx, m_full, path):
+        d, sigma, U, stamp = path.forward(m_full)
+        ctx.path, ctx.stamp = path, stamp
+        ctx.save_for_backward(m_full.detach(), sigma, U)
+        return d
+
+    @staticmethod
+    def backward(ctx, gd):
+        m_full, sigma, U = ctx.saved_tensors
+        path = ctx.path
+        path.ensure_factors(m_full, ctx.stamp)
+        return path.adjoint(gd, U, sigma).to(m_full.dtype), None

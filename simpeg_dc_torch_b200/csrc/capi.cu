@@ -1,0 +1,543 @@
+// C ABI of libdct: symbolic analysis handles, numeric plans (device buffers
+// and launch schedules), factorize / solve with float64 iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "dct_internal.h"
+
+using dct::Launch;
+using dct::PanelTask;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? DCT_ERR_OOM : DCT_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define DCT_CUDA(call, what)                              \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what);    \
+  } while (0)
+
+template <typename V>
+int upload(dct_plan* P, const std::vector<V>& h, const V** out) {
+  void* d = nullptr;
+  size_t bytes = std::max<size_t>(1, h.size() * sizeof(V));
+  cudaError_t e = cudaMalloc(&d, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (symbolic arrays)");
+  P->owned.push_back(d);
+  if (!h.empty()) {
+    e = cudaMemcpy(d, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy (symbolic arrays)");
+  }
+  *out = static_cast<const V*>(d);
+  return DCT_OK;
+}
+
+int alloc(dct_plan* P, size_t bytes, void** out, const char* what) {
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  P->owned.push_back(d);
+  *out = d;
+  return DCT_OK;
+}
+
+int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// ---- schedules ------------------------------------------------------------
+void build_factor_schedule(const dct::Symbolic& S, int small_max,
+                           dct::Schedule* out) {
+  auto& T = out->tasks;
+  auto& L = out->launches;
+  for (int lv = 0; lv < S.nlevels; ++lv) {
+    std::vector<int> small, large;
+    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+      int s = S.level_sn[q];
+      (S.front_n[s] <= small_max ? small : large).push_back(s);
+    }
+    if (!small.empty()) {
+      Launch l{dct::kSmallFront, lv, int64_t(T.size()), int64_t(small.size()), 0};
+      for (int s : small) {
+        T.push_back({s, 0, 0, 0});
+        l.arg = std::max(l.arg, S.front_n[s]);
+      }
+      L.push_back(l);
+    }
+    if (large.empty()) continue;
+    {
+      Launch l{dct::kLargeScatter, lv, int64_t(T.size()), int64_t(large.size()), 0};
+      for (int s : large) T.push_back({s, 0, 0, 0});
+      L.push_back(l);
+    }
+    int max_children = 0;
+    for (int s : large)
+      max_children = std::max(max_children, S.child_ptr[s + 1] - S.child_ptr[s]);
+    for (int slot = 0; slot < max_children; ++slot) {
+      Launch l{dct::kLargeExtendAdd, lv, int64_t(T.size()), 0, slot};
+      for (int s : large) {
+        int nch = S.child_ptr[s + 1] - S.child_ptr[s];
+        if (slot >= nch) continue;
+        int c = S.child[S.child_ptr[s] + slot];
+        int nbc = S.nb(c);
+        for (int j = 0; j < nbc; j += 8) T.push_back({s, 0, c, j});
+      }
+      l.count = int64_t(T.size()) - l.first;
+      L.push_back(l);
+    }
+    int max_panels = 0;
+    for (int s : large) max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
+    for (int p = 0; p < max_panels; ++p) {
+      Launch lp{dct::kLargePanel, lv, int64_t(T.size()), 0, p};
+      for (int s : large) {
+        int ns = S.ns(s), N = S.front_n[s];
+        int c0 = p * dct::kPanel;
+        if (c0 >= ns) continue;
+        int w = std::min(dct::kPanel, ns - c0);
+        int nt = ceil_div(N - c0 - w, dct::kPanel);
+        for (int t = 1; t <= nt; ++t) T.push_back({s, p, t, 0});
+      }
+      lp.count = int64_t(T.size()) - lp.first;
+      L.push_back(lp);
+      Launch lu{dct::kLargeUpdate, lv, int64_t(T.size()), 0, p};
+      for (int s : large) {
+        int ns = S.ns(s), N = S.front_n[s];
+        int c0 = p * dct::kPanel;
+        if (c0 >= ns) continue;
+        int w = std::min(dct::kPanel, ns - c0);
+        int nt = ceil_div(N - c0 - w, dct::kPanel);
+        T.push_back({s, p, -1, 0});
+        for (int i = 0; i < nt; ++i)
+          for (int j = 0; j <= i; ++j) T.push_back({s, p, i, j});
+      }
+      lu.count = int64_t(T.size()) - lu.first;
+      L.push_back(lu);
+    }
+  }
+}
+
+void build_solve_schedules(const dct::Symbolic& S, dct::Schedule* fwd,
+                           dct::Schedule* bwd) {
+  for (int lv = 0; lv < S.nlevels; ++lv) {
+    int max_panels = 0;
+    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q)
+      max_panels = std::max(max_panels, ceil_div(S.ns(S.level_sn[q]), dct::kPanel));
+    for (int p = 0; p < max_panels; ++p) {
+      Launch l{dct::kFwdStep, lv, int64_t(fwd->tasks.size()), 0, p};
+      for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+        int s = S.level_sn[q];
+        int ns = S.ns(s), N = S.front_n[s];
+        int c0 = p * dct::kPanel;
+        if (c0 >= ns) continue;
+        int w = std::min(dct::kPanel, ns - c0);
+        int nt = ceil_div(N - c0 - w, dct::kPanel);
+        for (int t = 0; t <= nt; ++t) fwd->tasks.push_back({s, p, t, 0});
+      }
+      l.count = int64_t(fwd->tasks.size()) - l.first;
+      fwd->launches.push_back(l);
+    }
+  }
+  for (int lv = S.nlevels - 1; lv >= 0; --lv) {
+    Launch lg{dct::kBwdGemm, lv, int64_t(bwd->tasks.size()), 0, 0};
+    int max_panels = 0;
+    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+      int s = S.level_sn[q];
+      int np = ceil_div(S.ns(s), dct::kPanel);
+      max_panels = std::max(max_panels, np);
+      if (S.nb(s) == 0) continue;
+      for (int p = 0; p < np; ++p) bwd->tasks.push_back({s, p, 0, 0});
+    }
+    lg.count = int64_t(bwd->tasks.size()) - lg.first;
+    bwd->launches.push_back(lg);
+    for (int p = max_panels - 1; p >= 0; --p) {
+      Launch l{dct::kBwdStep, lv, int64_t(bwd->tasks.size()), 0, p};
+      for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+        int s = S.level_sn[q];
+        if (p * dct::kPanel >= S.ns(s)) continue;
+        for (int i = 0; i <= p; ++i) bwd->tasks.push_back({s, p, i, 0});
+      }
+      l.count = int64_t(bwd->tasks.size()) - l.first;
+      bwd->launches.push_back(l);
+    }
+  }
+}
+
+int upload_schedule(dct_plan* P, dct::Schedule* sch) {
+  const PanelTask* d = nullptr;
+  int rc = upload(P, sch->tasks, &d);
+  sch->d_tasks = const_cast<PanelTask*>(d);
+  return rc;
+}
+
+size_t esize(int dtype) { return dtype == DCT_F64 ? 8 : 4; }
+
+int set_device(int device) {
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (cur != device) {
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  }
+  return DCT_OK;
+}
+
+}  // namespace
+
+void dct::set_last_error(const char* msg) { g_err = msg; }
+
+extern "C" {
+
+int dct_version(void) { return 10000; }
+
+const char* dct_last_error(void) { return g_err.c_str(); }
+
+int dct_symbolic_create(int32_t n, const int32_t* crow, const int32_t* col,
+                        const int32_t* coords, int32_t ndim, int32_t leaf_size,
+                        dct_symbolic** out) {
+  if (!out || !crow || !col || n <= 0) return fail(DCT_ERR_ARG, "bad arguments");
+  *out = nullptr;
+  auto* h = new (std::nothrow) dct_symbolic();
+  if (!h) return fail(DCT_ERR_OOM, "host allocation");
+  dct::SymbolicOptions opt;
+  if (leaf_size > 0) opt.leaf_size = leaf_size;
+  std::string why;
+  try {
+    why = dct::analyse(n, crow, col, coords, ndim, opt, &h->sym);
+  } catch (const std::exception& ex) {
+    delete h;
+    return fail(DCT_ERR_OOM, std::string("symbolic analysis: ") + ex.what());
+  }
+  if (!why.empty()) {
+    delete h;
+    return fail(DCT_ERR_BAD_PATTERN, why);
+  }
+  *out = h;
+  return DCT_OK;
+}
+
+void dct_symbolic_destroy(dct_symbolic* sym) { delete sym; }
+
+int dct_symbolic_get_info(const dct_symbolic* h, dct_symbolic_info* out) {
+  if (!h || !out) return fail(DCT_ERR_ARG, "null argument");
+  const dct::Symbolic& S = h->sym;
+  out->n = S.n;
+  out->nnz_in = S.nnz_in;
+  out->nsuper = S.nsuper;
+  out->nlevels = S.nlevels;
+  out->max_front = S.max_front;
+  out->max_ns = S.max_ns;
+  out->nnz_L = S.nnz_L;
+  out->front_total = S.front_total;
+  out->flops_factor = S.flops_factor;
+  return DCT_OK;
+}
+
+int dct_symbolic_get_array(const dct_symbolic* h, const char* name, void* dst,
+                           int64_t capacity_bytes, int64_t* size_bytes) {
+  if (!h || !name) return fail(DCT_ERR_ARG, "null argument");
+  const dct::Symbolic& S = h->sym;
+  const void* src = nullptr;
+  int64_t bytes = 0;
+  auto pick32 = [&](const std::vector<int32_t>& v) {
+    src = v.data();
+    bytes = int64_t(v.size()) * 4;
+  };
+  auto pick64 = [&](const std::vector<int64_t>& v) {
+    src = v.data();
+    bytes = int64_t(v.size()) * 8;
+  };
+  std::string nm(name);
+  if (nm == "perm") pick32(S.perm);
+  else if (nm == "iperm") pick32(S.iperm);
+  else if (nm == "sn_first") pick32(S.sn_first);
+  else if (nm == "sn_parent") pick32(S.sn_parent);
+  else if (nm == "sn_level") pick32(S.sn_level);
+  else if (nm == "front_n") pick32(S.front_n);
+  else if (nm == "front_off") pick64(S.front_off);
+  else if (nm == "rows_ptr") pick64(S.rows_ptr);
+  else if (nm == "rows") pick32(S.rows);
+  else if (nm == "child_ptr") pick32(S.child_ptr);
+  else if (nm == "child") pick32(S.child);
+  else if (nm == "rel_ptr") pick64(S.rel_ptr);
+  else if (nm == "rel") pick32(S.rel);
+  else if (nm == "amap_ptr") pick64(S.amap_ptr);
+  else if (nm == "amap_e") pick32(S.amap_e);
+  else if (nm == "amap_pos") pick32(S.amap_pos);
+  else return fail(DCT_ERR_ARG, "unknown array " + nm);
+  if (size_bytes) *size_bytes = bytes;
+  if (dst) {
+    if (capacity_bytes < bytes) return fail(DCT_ERR_ARG, "destination too small");
+    if (bytes) std::memcpy(dst, src, bytes);
+  }
+  return DCT_OK;
+}
+
+int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t which,
+                              int32_t* tasks, int64_t* ntasks, int64_t* launches,
+                              int64_t* nlaunches) {
+  if (!h || !ntasks || !nlaunches || which < 0 || which > 2 ||
+      (dtype != DCT_F64 && dtype != DCT_F32))
+    return fail(DCT_ERR_ARG, "bad arguments");
+  dct::Schedule f, fw, bw;
+  const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
+  build_factor_schedule(h->sym, small_max, &f);
+  build_solve_schedules(h->sym, &fw, &bw);
+  const dct::Schedule& sc = which == 0 ? f : (which == 1 ? fw : bw);
+  const int64_t nt = int64_t(sc.tasks.size()), nl = int64_t(sc.launches.size());
+  if (tasks) {
+    if (*ntasks < nt) return fail(DCT_ERR_ARG, "task buffer too small");
+    for (int64_t i = 0; i < nt; ++i) {
+      tasks[4 * i + 0] = sc.tasks[i].s;
+      tasks[4 * i + 1] = sc.tasks[i].p;
+      tasks[4 * i + 2] = sc.tasks[i].t0;
+      tasks[4 * i + 3] = sc.tasks[i].t1;
+    }
+  }
+  if (launches) {
+    if (*nlaunches < nl) return fail(DCT_ERR_ARG, "launch buffer too small");
+    for (int64_t i = 0; i < nl; ++i) {
+      const Launch& l = sc.launches[i];
+      launches[5 * i + 0] = l.kind;
+      launches[5 * i + 1] = l.level;
+      launches[5 * i + 2] = l.first;
+      launches[5 * i + 3] = l.count;
+      launches[5 * i + 4] = l.arg;
+    }
+  }
+  *ntasks = nt;
+  *nlaunches = nl;
+  return DCT_OK;
+}
+
+void dct_plan_destroy(dct_plan* P) {
+  if (!P) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  cudaSetDevice(P->device);
+  for (void* p : P->owned) cudaFree(p);
+  if (cur >= 0) cudaSetDevice(cur);
+  delete P;
+}
+
+int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
+                    int32_t dtype, int32_t device, dct_plan** out) {
+  if (!h || !out || nbatch < 1 || max_rhs < 1 ||
+      (dtype != DCT_F64 && dtype != DCT_F32))
+    return fail(DCT_ERR_ARG, "bad arguments");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(DCT_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(DCT_ERR_ARG, "bad device");
+  int rc = set_device(device);
+  if (rc) return rc;
+  auto* P = new (std::nothrow) dct_plan();
+  if (!P) return fail(DCT_ERR_OOM, "host allocation");
+  P->sym = h->sym;
+  P->device = device;
+  P->nbatch = nbatch;
+  P->max_rhs = max_rhs;
+  P->dtype = dtype;
+  const dct::Symbolic& S = P->sym;
+  auto bail = [&](int code) {
+    dct_plan_destroy(P);
+    return code;
+  };
+  dct::DevSym& D = P->ds;
+  if ((rc = upload(P, S.sn_first, &D.sn_first)) || (rc = upload(P, S.front_n, &D.front_n)) ||
+      (rc = upload(P, S.front_off, &D.front_off)) || (rc = upload(P, S.rows_ptr, &D.rows_ptr)) ||
+      (rc = upload(P, S.rows, &D.rows)) || (rc = upload(P, S.amap_ptr, &D.amap_ptr)) ||
+      (rc = upload(P, S.amap_e, &D.amap_e)) || (rc = upload(P, S.amap_pos, &D.amap_pos)) ||
+      (rc = upload(P, S.child_ptr, &D.child_ptr)) || (rc = upload(P, S.child, &D.child)) ||
+      (rc = upload(P, S.rel_ptr, &D.rel_ptr)) || (rc = upload(P, S.rel, &D.rel)) ||
+      (rc = upload(P, S.perm, &D.perm)) || (rc = upload(P, S.iperm, &D.iperm)) ||
+      (rc = upload(P, S.in_crow, &D.crow)) || (rc = upload(P, S.in_col, &D.col)))
+    return bail(rc);
+  const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
+  build_factor_schedule(S, small_max, &P->fact);
+  build_solve_schedules(S, &P->fwd, &P->bwd);
+  if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||
+      (rc = upload_schedule(P, &P->bwd)))
+    return bail(rc);
+  const size_t es = esize(dtype);
+  P->front_stride = S.front_total;
+  const size_t work = size_t(nbatch) * S.n * max_rhs;
+  void* p = nullptr;
+  if ((rc = alloc(P, es * S.front_total * nbatch, &P->fronts, "front storage")))
+    return bail(rc);
+  if ((rc = alloc(P, es * work, &P->bufA, "work buffer A"))) return bail(rc);
+  if ((rc = alloc(P, es * work, &P->bufB, "work buffer B"))) return bail(rc);
+  if (dtype == DCT_F32) {
+    if ((rc = alloc(P, 8 * work, &p, "refinement iterate"))) return bail(rc);
+    P->x64 = static_cast<double*>(p);
+    if ((rc = alloc(P, 8 * work, &p, "refinement rhs"))) return bail(rc);
+    P->b64 = static_cast<double*>(p);
+    if ((rc = alloc(P, 8 * size_t(nbatch) * S.nnz_in, &p, "float64 values")))
+      return bail(rc);
+    P->vals64 = static_cast<double*>(p);
+  }
+  if ((rc = alloc(P, 64, &p, "status"))) return bail(rc);
+  P->status = static_cast<int*>(p);
+  if ((rc = alloc(P, 16, &p, "residual"))) return bail(rc);
+  P->resid_bits = static_cast<unsigned long long*>(p);
+  if (cudaMemset(P->status, 0, 64) != cudaSuccess ||
+      cudaMemset(P->resid_bits, 0, 16) != cudaSuccess)
+    return bail(fail(DCT_ERR_CUDA, "cudaMemset"));
+  *out = P;
+  return DCT_OK;
+}
+
+int dct_plan_set_refinement(dct_plan* P, int32_t iterations) {
+  if (!P || iterations < 0) return fail(DCT_ERR_ARG, "bad arguments");
+  P->ir_iters = iterations;
+  return DCT_OK;
+}
+
+int dct_plan_iperm(const dct_plan* P, const int32_t** d_iperm) {
+  if (!P || !d_iperm) return fail(DCT_ERR_ARG, "null argument");
+  *d_iperm = P->ds.iperm;
+  return DCT_OK;
+}
+
+int64_t dct_plan_stamp(const dct_plan* P) { return P ? P->stamp : -1; }
+
+int dct_factorize(dct_plan* P, const void* d_vals, int32_t vals_dtype,
+                  int64_t vals_batch_stride, void* stream) {
+  if (!P || !d_vals || (vals_dtype != DCT_F64 && vals_dtype != DCT_F32))
+    return fail(DCT_ERR_ARG, "bad arguments");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (P->dtype == DCT_F32) {
+    // keep float64 values for the refinement residual
+    DCT_CUDA(dct::launch_convert_any(d_vals, vals_dtype, vals_batch_stride,
+                                     P->sym.nnz_in, P->nbatch, P->vals64,
+                                     DCT_F64, st),
+             "value copy");
+  }
+  DCT_CUDA(dct::run_factor(P, d_vals, vals_dtype, vals_batch_stride, st),
+           "factorization launch");
+  P->factored = 1;
+  ++P->stamp;
+  return DCT_OK;
+}
+
+namespace {
+
+// f32 plans: solve bp -> xp (both float64, permuted) with refinement.
+int solve_refined(dct_plan* P, const double* bp, int64_t bstride, int k,
+                  double* xp, cudaStream_t st) {
+  const int n = P->sym.n;
+  const int64_t per = int64_t(n) * k;
+  DCT_CUDA(cudaMemsetAsync(P->resid_bits, 0, 16, st), "memset");
+  DCT_CUDA(dct::launch_convert_any(bp, DCT_F64, bstride, per, P->nbatch, P->bufA,
+                                   DCT_F32, st),
+           "rhs conversion");
+  DCT_CUDA(dct::run_solve_f32(P, k, st), "solve launch");
+  DCT_CUDA(dct::launch_ir_update(P, xp, k, 1, st), "refinement update");
+  for (int it = 0; it < P->ir_iters; ++it) {
+    if (it + 1 == P->ir_iters) DCT_CUDA(cudaMemsetAsync(P->resid_bits, 0, 16, st), "memset");
+    DCT_CUDA(dct::launch_residual(P, bp, bstride, xp, k, st), "residual");
+    DCT_CUDA(dct::run_solve_f32(P, k, st), "solve launch");
+    DCT_CUDA(dct::launch_ir_update(P, xp, k, 0, st), "refinement update");
+  }
+  return DCT_OK;
+}
+
+}  // namespace
+
+int dct_solve_permuted(dct_plan* P, const double* d_bp, int32_t b_batched,
+                       int32_t k, double* d_xp, void* stream) {
+  if (!P || !d_bp || !d_xp || k < 1 || k > P->max_rhs)
+    return fail(DCT_ERR_ARG, "bad arguments");
+  if (!P->factored) return fail(DCT_ERR_NOT_FACTORED, "solve before factorize");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t per = int64_t(P->sym.n) * k;
+  const int64_t bstride = b_batched ? per : 0;
+  if (P->dtype == DCT_F64) {
+    if (d_bp != d_xp || !b_batched)
+      DCT_CUDA(dct::launch_convert_any(d_bp, DCT_F64, bstride, per, P->nbatch,
+                                       d_xp, DCT_F64, st),
+               "rhs copy");
+    DCT_CUDA(dct::run_solve_f64(P, d_xp, k, st), "solve launch");
+    return DCT_OK;
+  }
+  return solve_refined(P, d_bp, bstride, k, d_xp, st);
+}
+
+int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
+              int32_t k, void* d_x, void* stream) {
+  if (!P || !d_b || !d_x || k < 1 || k > P->max_rhs ||
+      (io_dtype != DCT_F64 && io_dtype != DCT_F32))
+    return fail(DCT_ERR_ARG, "bad arguments");
+  if (!P->factored) return fail(DCT_ERR_NOT_FACTORED, "solve before factorize");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int n = P->sym.n;
+  const int64_t per = int64_t(n) * k;
+  const int64_t bstride = b_batched ? per : 0;
+  if (P->dtype == DCT_F64) {
+    DCT_CUDA(dct::launch_perm_in_any(d_b, io_dtype, bstride, P->ds.perm, n, k,
+                                     P->nbatch, P->bufA, DCT_F64, st),
+             "permute rhs");
+    DCT_CUDA(dct::run_solve_f64(P, static_cast<double*>(P->bufA), k, st),
+             "solve launch");
+    DCT_CUDA(dct::launch_perm_out_any(P->bufA, DCT_F64, P->ds.perm, n, k,
+                                      P->nbatch, d_x, io_dtype, st),
+             "permute solution");
+    return DCT_OK;
+  }
+  DCT_CUDA(dct::launch_perm_in_any(d_b, io_dtype, bstride, P->ds.perm, n, k,
+                                   P->nbatch, P->b64, DCT_F64, st),
+           "permute rhs");
+  rc = solve_refined(P, P->b64, per, k, P->x64, st);
+  if (rc) return rc;
+  DCT_CUDA(dct::launch_perm_out_any(P->x64, DCT_F64, P->ds.perm, n, k, P->nbatch,
+                                    d_x, io_dtype, st),
+           "permute solution");
+  return DCT_OK;
+}
+
+int dct_check_status(dct_plan* P, void* stream, int32_t* code, int32_t* where,
+                     double* residual) {
+  if (!P) return fail(DCT_ERR_ARG, "null plan");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int hs[16] = {0};
+  unsigned long long rb[2] = {0, 0};
+  DCT_CUDA(cudaMemcpyAsync(hs, P->status, sizeof(hs), cudaMemcpyDeviceToHost, st),
+           "status read");
+  DCT_CUDA(cudaMemcpyAsync(rb, P->resid_bits, sizeof(rb), cudaMemcpyDeviceToHost, st),
+           "status read");
+  DCT_CUDA(cudaStreamSynchronize(st), "stream synchronize");
+  DCT_CUDA(cudaMemsetAsync(P->status, 0, 64, st), "status reset");
+  if (code) *code = hs[0];
+  if (where) *where = hs[0] ? hs[1] : -1;
+  if (residual) {
+    double r, b;
+    std::memcpy(&r, &rb[0], 8);
+    std::memcpy(&b, &rb[1], 8);
+    *residual = b > 0 ? r / b : 0.0;
+  }
+  return DCT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Internal declarations shared by the CUDA translation units of libdct.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/dct.h"
+#include "symbolic.h"
+
+namespace dct {
+
+// Device copy of the symbolic structure (plain pointers, passed by value).
+struct DevSym {
+  const int32_t* sn_first;
+  const int32_t* front_n;
+  const int64_t* front_off;
+  const int64_t* rows_ptr;
+  const int32_t* rows;
+  const int64_t* amap_ptr;
+  const int32_t* amap_e;
+  const int32_t* amap_pos;
+  const int32_t* child_ptr;
+  const int32_t* child;
+  const int64_t* rel_ptr;
+  const int32_t* rel;
+  const int32_t* perm;
+  const int32_t* iperm;
+  const int32_t* crow;   // input pattern (refinement residuals)
+  const int32_t* col;
+};
+
+// One launch of a factor or solve schedule: `count` tasks from `first`.
+struct Launch {
+  int kind;
+  int level;
+  int64_t first;
+  int64_t count;
+  int arg;         // small fronts: largest front order of the launch
+};
+
+enum LaunchKind : int {
+  kSmallFront = 0,   // fused assemble + partial Cholesky, one CTA per front
+  kLargeScatter,     // matrix entries into large fronts
+  kLargeExtendAdd,   // one child slot into large fronts
+  kLargePanel,       // diagonal block Cholesky + TRSM of the rows below
+  kLargeUpdate,      // trailing symmetric update tiles
+  kFwdStep,          // forward substitution, one panel step
+  kBwdGemm,          // backward: subtract boundary-row contributions
+  kBwdStep,          // backward substitution, one panel step
+};
+
+// Limits of the single-CTA front kernel (front fully in shared memory).
+constexpr int kSmallFrontF64 = 160;
+constexpr int kSmallFrontF32 = 224;
+constexpr int kThreads = 256;
+constexpr int kRhsChunk = 32;   // right-hand sides per CTA in the solves
+
+struct Schedule {
+  std::vector<PanelTask> tasks;    // host copy
+  PanelTask* d_tasks = nullptr;    // device copy
+  std::vector<Launch> launches;
+};
+
+}  // namespace dct
+
+// The plan object behind the opaque handle of the C ABI.
+struct dct_plan {
+  dct::Symbolic sym;
+  int device = 0;
+  int nbatch = 1;
+  int max_rhs = 1;
+  int dtype = DCT_F64;             // factor / solve precision
+  dct::DevSym ds{};
+  std::vector<void*> owned;        // device allocations
+  void* fronts = nullptr;          // nbatch * front_total elements of dtype
+  int64_t front_stride = 0;
+  dct::Schedule fact;              // factorization schedule
+  dct::Schedule fwd;               // forward substitution schedule
+  dct::Schedule bwd;               // backward substitution schedule
+  void* bufA = nullptr;            // dtype, nbatch*n*max_rhs (work buffer A)
+  void* bufB = nullptr;            // dtype, nbatch*n*max_rhs (work buffer B)
+  double* x64 = nullptr;           // f32 plans: refined solution (dct_solve)
+  double* b64 = nullptr;           // f32 plans: permuted rhs (dct_solve)
+  double* vals64 = nullptr;        // f32 plans: float64 values (residuals)
+  int* status = nullptr;           // device: code, supernode, system
+  unsigned long long* resid_bits = nullptr;  // device: max|r|, max|b|
+  int factored = 0;
+  int64_t stamp = 0;
+  int ir_iters = 2;                // refinement iterations of f32 plans
+};
+
+struct dct_symbolic {
+  dct::Symbolic sym;
+};
+
+namespace dct {
+// records the message returned by dct_last_error() for this thread
+void set_last_error(const char* msg);
+cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,
+                       int64_t vals_stride, cudaStream_t st);
+cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st);
+cudaError_t run_solve_f32(dct_plan* P, int k, cudaStream_t st);
+cudaError_t launch_perm_in_any(const void* b, int b_dtype, int64_t bstride,
+                               const int32_t* perm, int n, int k, int nbatch,
+                               void* dst, int dst_dtype, cudaStream_t st);
+cudaError_t launch_perm_out_any(const void* src, int src_dtype,
+                                const int32_t* perm, int n, int k, int nbatch,
+                                void* x, int x_dtype, cudaStream_t st);
+cudaError_t launch_convert_any(const void* src, int src_dtype, int64_t sstride,
+                               int64_t count, int nbatch, void* dst,
+                               int dst_dtype, cudaStream_t st);
+cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
+                            const double* x, int k, cudaStream_t st);
+cudaError_t launch_ir_update(dct_plan* P, double* x, int k, int first,
+                             cudaStream_t st);
+}  // namespace dct

@@ -1,0 +1,206 @@
+"""Differentiable 2.5-D DC resistivity on a B200 (drop-in for dctorch's
+`TorchDC2D`, dctorch/simulation2d.py:34-534).
+
+The constructor, `dpred`, `misfit`, `misfit_and_grad` and `Jtvec` keep the
+reference's signatures and results.  At build time the sigma-linear maps
+L_ky, the sources q, the receiver projection Pd and the wavenumber quadrature
+are assembled from the mesh (see `operators.py` and `quadrature.py`); at run
+time the whole forward + adjoint chain runs in the hand-written CUDA kernels
+of libdct (see `_fused.py`): all nky wavenumbers and all sources are factored
+and solved in the same launches.
+
+Precision: `dtype=torch.float64` (default) factors and solves in float64;
+`dtype=torch.float32` factors and solves in float32 with float64 iterative
+refinement (`refine` iterations, default 2).  The quadrature sum, the data
+and the misfit are float64 in both.  Data come back in the model's dtype.
+
+Not provided (out of this package's scope): singularity removal and SimPEG's
+own wavenumber fit (`quadrature="simpeg"`), both of which need SimPEG.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from ._fused import FusedDpred, FusedPath
+from .operators import nodal_operators
+from .quadrature import (amplification, electrode_distance_range,
+                         k0_quadrature, transform_error)
+
+
+def _to_coo_tensor(M, device, dtype):
+    M = sp.coo_matrix(M)
+    return torch.sparse_coo_tensor(
+        torch.as_tensor(np.vstack((M.row, M.col)), dtype=torch.int64,
+                        device=device),
+        torch.as_tensor(M.data, dtype=dtype, device=device),
+        M.shape).coalesce()
+
+
+class _ActiveCells:
+    """m_full = P m + v_inactive (dctorch/simulation2d.py:122-134, 299-304)."""
+
+    def __init__(self, active_cells, val_inactive, nC, device):
+        act = np.asarray(active_cells, dtype=bool)
+        if act.size != nC:
+            raise ValueError("active_cells must have one entry per cell")
+        self.idx = torch.as_tensor(np.where(act)[0], device=device)
+        v = np.full(nC, float(val_inactive))
+        v[act] = 0.0
+        self.v = torch.as_tensor(v, dtype=torch.float64, device=device)
+        self.nA = int(act.sum())
+
+    def full(self, m):
+        return self.v.to(m.dtype).index_add(0, self.idx, m)
+
+    def restrict(self, g_full):
+        return g_full[self.idx]
+
+
+class TorchDC2D:
+    """Differentiable dpred/misfit for 2.5-D nodal DC on a fixed mesh+survey."""
+
+    def __init__(self, mesh, survey, nky=12, device="cuda",
+                 dtype=torch.float64, active_cells=None, val_inactive=None,
+                 chunk=None, singularity_removal=False, rho_primary=None,
+                 quadrature=None, refine=None):
+        if singularity_removal:
+            raise NotImplementedError(
+                "singularity removal is not part of this implementation")
+        if quadrature is None:
+            quadrature = os.environ.get("DCTORCH_QUADRATURE", "electrodes")
+        if isinstance(quadrature, str) and quadrature != "electrodes":
+            raise NotImplementedError(
+                f"quadrature={quadrature!r} needs SimPEG's own wavenumber fit; "
+                "use 'electrodes' or pass (points, weights)")
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise NotImplementedError("TorchDC2D here runs on CUDA devices only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.dtype = dtype
+        self.chunk = None if chunk is None else int(chunk)
+        self._sr = False
+
+        rmin, rmax = electrode_distance_range(survey)
+        if isinstance(quadrature, str):
+            kys, wq, info = k0_quadrature(rmin, rmax, nky)
+            self.quadrature_info = {
+                "source": "electrodes", "r_range": (rmin, rmax),
+                "max_rel_err": info["max_rel_err"],
+                "amplification": info["amplification"],
+                "n_used": info["n_used"]}
+        else:
+            kys, wq = (np.asarray(a, float) for a in quadrature)
+            self.quadrature_info = {
+                "source": "given", "r_range": (rmin, rmax),
+                "max_rel_err": transform_error(kys, wq, rmin, rmax),
+                "amplification": amplification(wq), "n_used": int(kys.size)}
+
+        ops = nodal_operators(mesh, survey)
+        self._ops = ops
+        self.kys = np.asarray(kys, float)
+        self.wq_np = np.asarray(wq, float)
+        self.nC, self.nN, self.nS, self.nD = ops.nC, ops.nN, ops.nS, ops.nD
+        self.nky = int(self.kys.size)
+        self.nnzA = ops.nnzA
+        L = sp.vstack([ops.L_ky(k) for k in self.kys]).tocsr()
+        self._L = L
+        self._check_symmetric(L)
+        precision = "fp64" if dtype == torch.float64 else "fp32_ir"
+        self.precision = precision
+        self._path = FusedPath(ops.crow, ops.col, L, self.wq_np, ops.q, ops.Pd,
+                               ops.sidx, self.device, precision,
+                               coords=mesh.node_grid_index()
+                               if hasattr(mesh, "node_grid_index") else None,
+                               refine=refine)
+        self.solver = self._path.solver
+        self.sidx = torch.as_tensor(ops.sidx, device=self.device)
+        self.iD = torch.arange(self.nD, device=self.device)
+        self.wq = torch.as_tensor(self.wq_np, dtype=torch.float64,
+                                  device=self.device)
+        self._inj = None
+        if active_cells is not None:
+            self._inj = _ActiveCells(active_cells, val_inactive, self.nC,
+                                     self.device)
+        self._mesh, self._survey = mesh, survey
+        self._lstack = None
+
+    # ------------------------------------------------------------ helpers
+    def _check_symmetric(self, L):
+        """The factorization is Cholesky: A must be symmetric for every ky
+        (checked once at build time at a reference model)."""
+        sig = np.full(self.nC, 0.01)
+        v = L[:self.nnzA] @ sig
+        A = sp.csr_matrix((v, self._ops.col, self._ops.crow),
+                          shape=(self.nN, self.nN))
+        if abs(A - A.T).max() > 1e-12 * abs(A).max():
+            raise ValueError("assembled operator is not symmetric")
+
+    @property
+    def Lstack(self):
+        """The stacked assembly map (nky*nnzA, nC) as a torch sparse tensor
+        (the reference engine's attribute)."""
+        if self._lstack is None:
+            self._lstack = _to_coo_tensor(self._L, self.device, torch.float64)
+        return self._lstack
+
+    @property
+    def q(self):
+        return torch.as_tensor(self._ops.q.toarray(), dtype=torch.float64,
+                               device=self.device)
+
+    @property
+    def Pd(self):
+        return _to_coo_tensor(self._ops.Pd, self.device, torch.float64)
+
+    def _model_to_full(self, m):
+        m_loc = m.to(device=self.device, dtype=torch.float64).reshape(-1)
+        if self._inj is not None:
+            m_loc = self._inj.full(m_loc)
+        return m_loc
+
+    def _grad_to_model(self, g_full, m):
+        g = g_full if self._inj is None else self._inj.restrict(g_full)
+        return g.to(device=m.device, dtype=m.dtype)
+
+    # ------------------------------------------------------------ runtime
+    def dpred(self, m):
+        """Predicted data (nD,) for m = log(rho). Autograd-traceable."""
+        dev0, dt0 = m.device, m.dtype
+        m_full = self._model_to_full(m)
+        d = FusedDpred.apply(m_full, self._path)
+        return d.to(device=dev0, dtype=dt0)
+
+    def misfit(self, m, dobs, w):
+        """phi_d = ||w*(dpred-dobs)||^2 (no 1/2 factor)."""
+        r = w * (self.dpred(m) - dobs)
+        return (r ** 2).sum()
+
+    def misfit_and_grad(self, m, dobs, w, chunk=None):
+        """(phi_d, dphi_d/dm) outside the autograd graph
+        (dctorch/simulation2d.py:345-375).  All sources are solved against one
+        factorization; `chunk` is accepted for compatibility."""
+        with torch.no_grad():
+            m_full = self._model_to_full(m)
+            d, sigma, U, _ = self._path.forward(m_full)
+            wd = w.to(self.device, torch.float64)
+            r = wd * (d - dobs.to(self.device, torch.float64))
+            phi = (r ** 2).sum()
+            g = self._path.adjoint(2.0 * wd * r, U, sigma)
+        return float(phi), self._grad_to_model(g, m)
+
+    def Jtvec(self, m, v, chunk=None):
+        """J^T v without forming J (dctorch/simulation2d.py:398-437)."""
+        with torch.no_grad():
+            m_full = self._model_to_full(m)
+            _, sigma, U, _ = self._path.forward(m_full)
+            g = self._path.adjoint(v.reshape(-1), U, sigma)
+        return self._grad_to_model(g, m)
+
+    def check(self):
+        """Synchronise and raise if a kernel reported an error."""
+        return self.solver.check()

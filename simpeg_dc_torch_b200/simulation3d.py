@@ -1,0 +1,115 @@
+"""Differentiable 3-D DC resistivity on a B200 (drop-in for dctorch's
+`TorchDC3D`, dctorch/simulation3d.py:44-227).
+
+Same recipe as the 2.5-D engine without wavenumbers: one assembly map
+L3 = L_edge + L_bc (Robin), one system factored once per evaluation, all
+sources solved as right-hand sides of that factorization, and the adjoint
+reusing it.  `dtype=torch.float32` selects the float32 factor/solve with
+float64 iterative refinement; data and misfit are float64 either way.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from ._fused import FusedDpred, FusedPath
+from .operators import nodal_operators
+from .simulation2d import _ActiveCells, _to_coo_tensor
+
+
+class TorchDC3D:
+    """Differentiable dpred/misfit for 3-D nodal DC on a fixed mesh+survey."""
+
+    def __init__(self, mesh, survey, device="cuda", dtype=torch.float64,
+                 active_cells=None, val_inactive=None, bc_type="Robin",
+                 refine=None):
+        if bc_type != "Robin":
+            raise NotImplementedError("only the Robin boundary condition is built")
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise NotImplementedError("TorchDC3D here runs on CUDA devices only")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.dtype = dtype
+        ops = nodal_operators(mesh, survey)
+        self._ops = ops
+        self.nC, self.nN, self.nS, self.nD = ops.nC, ops.nN, ops.nS, ops.nD
+        self.nnzA = ops.nnzA
+        L3 = ops.L3()
+        self._L = L3
+        A = sp.csr_matrix((L3 @ np.full(self.nC, 0.01), ops.col, ops.crow),
+                          shape=(self.nN, self.nN))
+        if abs(A - A.T).max() > 1e-12 * abs(A).max():
+            raise ValueError("assembled operator is not symmetric")
+        self.precision = "fp64" if dtype == torch.float64 else "fp32_ir"
+        self._path = FusedPath(ops.crow, ops.col, L3, None, ops.q, ops.Pd,
+                               ops.sidx, self.device, self.precision,
+                               coords=mesh.node_grid_index()
+                               if hasattr(mesh, "node_grid_index") else None,
+                               refine=refine)
+        self.solver = self._path.solver
+        self.sidx = torch.as_tensor(ops.sidx, device=self.device)
+        self.iD = torch.arange(self.nD, device=self.device)
+        self._inj = None
+        if active_cells is not None:
+            self._inj = _ActiveCells(active_cells, val_inactive, self.nC,
+                                     self.device)
+        self._l3 = None
+
+    @property
+    def L3(self):
+        if self._l3 is None:
+            self._l3 = _to_coo_tensor(self._L, self.device, torch.float64)
+        return self._l3
+
+    @property
+    def q(self):
+        return torch.as_tensor(self._ops.q.toarray(), dtype=torch.float64,
+                               device=self.device)
+
+    @property
+    def Pd(self):
+        return _to_coo_tensor(self._ops.Pd, self.device, torch.float64)
+
+    def _model_to_full(self, m):
+        m_loc = m.to(device=self.device, dtype=torch.float64).reshape(-1)
+        if self._inj is not None:
+            m_loc = self._inj.full(m_loc)
+        return m_loc
+
+    def _grad_to_model(self, g_full, m):
+        g = g_full if self._inj is None else self._inj.restrict(g_full)
+        return g.to(device=m.device, dtype=m.dtype)
+
+    def dpred(self, m):
+        """Predicted data (nD,) for m = log(rho). Autograd-traceable."""
+        dev0, dt0 = m.device, m.dtype
+        d = FusedDpred.apply(self._model_to_full(m), self._path)
+        return d.to(device=dev0, dtype=dt0)
+
+    def Jtvec(self, m, v):
+        """J^T v (dctorch/simulation3d.py:209-222)."""
+        with torch.no_grad():
+            m_full = self._model_to_full(m)
+            _, sigma, U, _ = self._path.forward(m_full)
+            g = self._path.adjoint(v.reshape(-1), U, sigma)
+        return self._grad_to_model(g, m)
+
+    def misfit(self, m, dobs, w):
+        """phi_d = ||w*(dpred-dobs)||^2."""
+        r = w * (self.dpred(m) - dobs)
+        return (r ** 2).sum()
+
+    def misfit_and_grad(self, m, dobs, w):
+        with torch.no_grad():
+            m_full = self._model_to_full(m)
+            d, sigma, U, _ = self._path.forward(m_full)
+            wd = w.to(self.device, torch.float64)
+            r = wd * (d - dobs.to(self.device, torch.float64))
+            phi = (r ** 2).sum()
+            g = self._path.adjoint(2.0 * wd * r, U, sigma)
+        return float(phi), self._grad_to_model(g, m)
+
+    def check(self):
+        return self.solver.check()

@@ -1,0 +1,310 @@
+"""Sparse SPD direct solve on a B200 as torch autograd ops (drop-in for
+dctorch/solver.py on CUDA devices).
+
+The classes mirror the reference's solver surface: `DCTSolver` replaces
+`CuDSSSolver` (dctorch/solver.py:76-138), `DCTBatchSolver` replaces
+`CuDSSBatchSolver` (dctorch/solver.py:181-233); `make_solver` and
+`make_batch_solver` (dctorch/solver.py:383-399) return them for CUDA devices.
+Attributes `n, n_rhs, nbatch, device, dtype, crow, col, row, stamp` and methods
+`factorize(values)`, `solve(b)`, `free()` keep the reference's meaning and
+shapes.  The symbolic analysis (nested dissection + assembly tree) runs once
+per instance; `factorize` is a numeric refactorization of new values on the
+same pattern.
+
+Precision: a float64 solver factors and solves in float64.  A float32 solver
+factors and solves in float32 and refines every solution with residuals
+b - A x formed in float64 (`refine` iterations, default 2; 0 gives the plain
+float32 solve of the reference).
+
+The differentiable ops `sparse_solve`, `sparse_solve_batch` and
+`sparse_solve_batch_prefactored` have the reference's contract
+(dctorch/solver.py:141-178, 236-311): the backward solves the adjoint on the
+same factors (A symmetric) and contracts it with the solution on the pattern,
+grad_vals[e] = -sum_s adj[row_e, s] x[col_e, s], here in one CUDA kernel.
+
+Only CUDA devices are served; there is no CPU path in this package.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _native as nat
+
+_MATRIX_TYPES = ("spd",)
+
+
+def _require_cuda(device):
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise NotImplementedError(
+            "simpeg_dc_torch_b200 implements the CUDA solver path only; "
+            f"got device {device}")
+    if not torch.cuda.is_available():
+        raise RuntimeError("a CUDA device was requested but none is available")
+    if device.index is None:
+        device = torch.device("cuda", torch.cuda.current_device())
+    return device
+
+
+def _stream_ptr(device):
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _dtype_code(dt):
+    if dt == torch.float64:
+        return nat.F64
+    if dt == torch.float32:
+        return nat.F32
+    raise TypeError(f"unsupported dtype {dt}; float64 or float32 expected")
+
+
+class _PlanSolver:
+    """Shared machinery of the single and batched solvers."""
+
+    def __init__(self, crow, col, n, n_rhs, nbatch, device, dtype,
+                 matrix_type, coords, refine, leaf_size):
+        if matrix_type not in _MATRIX_TYPES:
+            raise NotImplementedError(
+                f"matrix_type {matrix_type!r}: only real SPD systems are "
+                "factored here (Cholesky)")
+        self.device = _require_cuda(device)
+        self.dtype = dtype
+        self._code = _dtype_code(dtype)
+        self.n, self.n_rhs, self.nbatch = int(n), int(n_rhs), int(nbatch)
+        crow_np = np.asarray(torch.as_tensor(crow).cpu().numpy(), dtype=np.int32)
+        col_np = np.asarray(torch.as_tensor(col).cpu().numpy(), dtype=np.int32)
+        if crow_np.size != self.n + 1:
+            raise ValueError("crow must have n+1 entries")
+        self.crow = torch.as_tensor(crow_np).to(self.device)
+        self.col = torch.as_tensor(col_np).to(self.device)
+        counts = self.crow[1:] - self.crow[:-1]
+        self.row = torch.repeat_interleave(
+            torch.arange(self.n, device=self.device, dtype=torch.int32),
+            counts)
+        self.nnz = int(col_np.size)
+        self._sym = nat.Symbolic(crow_np, col_np, coords, leaf_size)
+        with torch.cuda.device(self.device):
+            self._plan = nat.Plan(self._sym, self.nbatch, self.n_rhs,
+                                  self._code, self.device.index)
+        if refine is not None:
+            self._plan.set_refinement(int(refine))
+        self.stamp = 0
+
+    # ---- introspection
+    @property
+    def plan(self):
+        return self._plan
+
+    def analysis(self):
+        """Statistics of the symbolic analysis (fronts, nnz(L), flops)."""
+        return self._sym.info()
+
+    def check(self):
+        """Synchronise and raise if a kernel reported an error (for example a
+        non-positive pivot).  Returns the last refinement residual ratio."""
+        code, where, res = self._plan.status(_stream_ptr(self.device))
+        if code != 0:
+            raise nat.DCTError(code, "factorization", f"at supernode {where}")
+        return res
+
+    # ---- numeric phases
+    def _factorize(self, values):
+        v = values.detach()
+        if v.dtype not in (torch.float64, torch.float32):
+            v = v.to(torch.float64)
+        v = v.to(self.device).contiguous()
+        if v.dim() == 1:
+            v = v.unsqueeze(0)
+        if v.shape != (self.nbatch, self.nnz):
+            raise ValueError(f"values must be ({self.nbatch}, {self.nnz}), "
+                             f"got {tuple(v.shape)}")
+        self._plan.factorize(v.data_ptr(), _dtype_code(v.dtype), self.nnz,
+                             _stream_ptr(self.device))
+        self._vals_keepalive = v
+        self.stamp += 1
+
+    def _solve(self, b2, batched):
+        """b2: (n, k) or (nbatch, n, k) in self.dtype; returns (nbatch, n, k)."""
+        k = b2.shape[-1]
+        if k > self.n_rhs:
+            raise ValueError(f"{k} right-hand sides exceed n_rhs={self.n_rhs}")
+        x = torch.empty((self.nbatch, self.n, k), dtype=self.dtype,
+                        device=self.device)
+        self._plan.solve(b2.data_ptr(), self._code, 1 if batched else 0, k,
+                         x.data_ptr(), _stream_ptr(self.device))
+        return x
+
+    def free(self):
+        if getattr(self, "_plan", None) is not None:
+            self._plan.free()
+            self._plan = None
+
+
+class DCTSolver(_PlanSolver):
+    """Stateful SPD solver bound to one pattern and RHS width
+    (the interface of dctorch's CuDSSSolver)."""
+
+    def __init__(self, crow, col, n, n_rhs, device="cuda",
+                 dtype=torch.float64, matrix_type="spd", coords=None,
+                 refine=None, leaf_size=64):
+        super().__init__(crow, col, n, n_rhs, 1, device, dtype, matrix_type,
+                         coords, refine, leaf_size)
+
+    def factorize(self, values):
+        """Numeric refactorization with new values (nnz,), same pattern."""
+        self._factorize(values.reshape(1, -1))
+
+    def solve(self, b):
+        """Solve A x = b for the current factorization; b (n,) or (n, k)."""
+        b2 = b.detach().to(device=self.device, dtype=self.dtype)
+        b2 = b2.reshape(self.n, -1).contiguous()
+        x = self._solve(b2, False)
+        return x[0].reshape(b.shape)
+
+
+class DCTBatchSolver(_PlanSolver):
+    """`nbatch` SPD systems on one shared pattern (the interface of dctorch's
+    CuDSSBatchSolver): one analysis, every system factored and solved in the
+    same launches."""
+
+    def __init__(self, crow, col, n, n_rhs, nbatch, device="cuda",
+                 dtype=torch.float64, matrix_type="spd", coords=None,
+                 refine=None, leaf_size=64):
+        super().__init__(crow, col, n, n_rhs, nbatch, device, dtype,
+                         matrix_type, coords, refine, leaf_size)
+
+    def factorize(self, values):
+        """values: (nbatch, nnz) -- refactorize every system."""
+        self._factorize(values)
+
+    def solve(self, b):
+        """b: (nbatch, n, k) or shared (n, k); returns (nbatch, n, k)."""
+        shared = b.dim() == 2
+        b2 = b.detach().to(device=self.device, dtype=self.dtype).contiguous()
+        return self._solve(b2, not shared)
+
+
+# --------------------------------------------------------------- autograd
+def _grad_vals(solver, adj, x):
+    """-sum_s adj[b, row_e, s] x[b, col_e, s] for every pattern entry."""
+    nb = adj.shape[0]
+    k = adj.shape[-1]
+    out = torch.empty((nb, solver.nnz), dtype=adj.dtype, device=adj.device)
+    nat.check(nat.lib().dct_gather_contract_plain(
+        nb, solver.n, solver.nnz, k, solver.row.data_ptr(),
+        solver.col.data_ptr(), _dtype_code(adj.dtype),
+        adj.contiguous().data_ptr(), x.contiguous().data_ptr(),
+        out.data_ptr(), _stream_ptr(solver.device)), "gather_contract")
+    return out
+
+
+class _SparseSolveFn(torch.autograd.Function):
+    """x = A(values)^{-1} b, differentiable in values and b (A SPD)."""
+
+    @staticmethod
+    def forward(ctx, values, b, solver):
+        solver.factorize(values.detach())
+        x = solver.solve(b.detach())
+        ctx.solver = solver
+        ctx.dt_vals, ctx.dt_b = values.dtype, b.dtype
+        ctx.save_for_backward(x)
+        return x
+
+    @staticmethod
+    def backward(ctx, grad_x):
+        (x,) = ctx.saved_tensors
+        solver = ctx.solver
+        adj = solver.solve(grad_x.contiguous())
+        grad_vals = grad_b = None
+        if ctx.needs_input_grad[0]:
+            gv = _grad_vals(solver, adj.reshape(1, solver.n, -1),
+                            x.reshape(1, solver.n, -1))
+            grad_vals = gv[0].to(ctx.dt_vals)
+        if ctx.needs_input_grad[1]:
+            grad_b = adj.to(ctx.dt_b)
+        return grad_vals, grad_b, None
+
+
+def sparse_solve(values, b, solver):
+    """Differentiable sparse SPD solve (dctorch/solver.py:176-178)."""
+    return _SparseSolveFn.apply(values, b, solver)
+
+
+class _SparseSolveBatchFn(torch.autograd.Function):
+    """x_i = A_i(values_i)^{-1} b on one shared pattern (real SPD)."""
+
+    @staticmethod
+    def forward(ctx, values, b, solver):
+        solver.factorize(values.detach())
+        x = solver.solve(b.detach())
+        ctx.solver = solver
+        ctx.b_shared = b.dim() == 2
+        ctx.dt_vals, ctx.dt_b = values.dtype, b.dtype
+        ctx.save_for_backward(x)
+        return x
+
+    @staticmethod
+    def backward(ctx, grad_x):
+        (x,) = ctx.saved_tensors
+        solver = ctx.solver
+        adj = solver.solve(grad_x.contiguous())
+        grad_vals = grad_b = None
+        if ctx.needs_input_grad[0]:
+            grad_vals = _grad_vals(solver, adj, x).to(ctx.dt_vals)
+        if ctx.needs_input_grad[1]:
+            gb = adj.sum(0) if ctx.b_shared else adj
+            grad_b = gb.to(ctx.dt_b)
+        return grad_vals, grad_b, None
+
+
+class _SparseSolveBatchPreFn(torch.autograd.Function):
+    """As _SparseSolveBatchFn for an A the caller already factorized."""
+
+    @staticmethod
+    def forward(ctx, values, b, solver):
+        x = solver.solve(b.detach())
+        ctx.solver = solver
+        ctx.b_shared = b.dim() == 2
+        ctx.dt_vals, ctx.dt_b = values.dtype, b.dtype
+        ctx.save_for_backward(x)
+        return x
+
+    backward = _SparseSolveBatchFn.backward
+
+
+def sparse_solve_batch(values, b, solver):
+    """values: (nbatch, nnz) | b: (nbatch, n, k) or shared (n, k)."""
+    return _SparseSolveBatchFn.apply(values, b, solver)
+
+
+def sparse_solve_batch_prefactored(values, b, solver):
+    """Differentiable solve on an already-factorized A."""
+    return _SparseSolveBatchPreFn.apply(values, b, solver)
+
+
+def _default_mtype(dtype, matrix_type):
+    if matrix_type is not None:
+        return matrix_type
+    return "symmetric" if dtype.is_complex else "spd"
+
+
+def make_solver(crow, col, n, n_rhs, device="cuda", dtype=torch.float64,
+                matrix_type=None, **kw):
+    """Factory (dctorch/solver.py:383-390): the B200 solver for CUDA devices."""
+    mt = _default_mtype(dtype, matrix_type)
+    return DCTSolver(crow, col, n, n_rhs, device=device, dtype=dtype,
+                     matrix_type=mt, **kw)
+
+
+def make_batch_solver(crow, col, n, n_rhs, nbatch, device="cuda",
+                      dtype=torch.float64, matrix_type=None, **kw):
+    """Factory (dctorch/solver.py:393-399)."""
+    mt = _default_mtype(dtype, matrix_type)
+    return DCTBatchSolver(crow, col, n, n_rhs, nbatch, device=device,
+                          dtype=dtype, matrix_type=mt, **kw)
+
+
+# the reference's class names, for `from ... import CuDSSSolver` call sites
+CuDSSSolver = DCTSolver
+CuDSSBatchSolver = DCTBatchSolver

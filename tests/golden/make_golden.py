@@ -1,0 +1,235 @@
+"""Generate the golden fixtures from the reference implementation itself.
+
+Run in a container that holds the reference source tree:
+
+    python tests/golden/make_golden.py --reference /path/to/SimPEG_DC_Torch
+
+The reference's runtime modules (dctorch/solver.py, quadrature.py,
+simulation2d.py, simulation3d.py) are loaded under a stub `dctorch` package
+that skips dctorch/__init__.py (which imports SimPEG, absent here).  Engines
+are made with `object.__new__` and given this package's operators; every
+output below is computed by the reference's own code on its CPU (SuperLU)
+path in float64:
+
+  solver_nx12.npz / solver_nx40.npz : dctorch.solver.sparse_solve on the
+      5-point Laplacian + 0.1 I of dctorch/tests/test_solver.py:19-25, with
+      the value/rhs gradients of loss = sum(w * x).
+  quad.npz        : dctorch.quadrature.k0_quadrature points and weights.
+  dc2d_tiny.npz   : a 24x12-cell 2.5-D problem, all operators stored, with
+      dpred, misfit, misfit gradient, Jtvec, chunked Jtvec and
+      misfit_and_grad from TorchDC2D.
+  dc2d_suite.npz  : the reference suite's 2-D tensor case
+      (dctorch/tests/test_suite.py:65-67), outputs + operator checksums.
+  dc3d_tiny.npz / dc3d_suite.npz : the same for TorchDC3D.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import types
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+from simpeg_dc_torch_b200 import synthetic as syn  # noqa: E402
+from simpeg_dc_torch_b200.operators import nodal_operators  # noqa: E402
+from simpeg_dc_torch_b200.quadrature import (  # noqa: E402
+    electrode_distance_range)
+
+
+def load_reference(root):
+    pkg = types.ModuleType("dctorch")
+    pkg.__path__ = [os.path.join(root, "dctorch")]
+    sys.modules["dctorch"] = pkg
+    import dctorch.quadrature as Q
+    import dctorch.simulation2d as S2
+    import dctorch.simulation3d as S3
+    import dctorch.solver as S
+    return S, Q, S2, S3
+
+
+def laplacian(nx):
+    T = sp.diags([-1.0, 2.0, -1.0], [-1, 0, 1], shape=(nx, nx))
+    I = sp.eye(nx)
+    A = (sp.kron(I, T) + sp.kron(T, I) + 0.1 * sp.eye(nx * nx)).tocsr()
+    A.sort_indices()
+    return A
+
+
+def solver_fixture(S, nx, n_rhs, seed):
+    A = laplacian(nx)
+    n = A.shape[0]
+    rng = np.random.default_rng(seed)
+    b = rng.standard_normal((n, n_rhs))
+    w = rng.standard_normal((n, n_rhs))
+    slv = S.SciPySolver(torch.tensor(A.indptr, dtype=torch.int32),
+                        torch.tensor(A.indices, dtype=torch.int32), n, n_rhs)
+    vals = torch.tensor(A.data, requires_grad=True)
+    bt = torch.tensor(b, requires_grad=True)
+    x = S.sparse_solve(vals, bt, slv)
+    (torch.tensor(w) * x).sum().backward()
+    return dict(crow=A.indptr.astype(np.int32), col=A.indices.astype(np.int32),
+                vals=A.data, b=b, w=w, x=x.detach().numpy(),
+                grad_vals=vals.grad.numpy(), grad_b=bt.grad.numpy())
+
+
+def engine_2d(S2, ops, kys, wq, chunk=None):
+    L = sp.vstack([ops.L_ky(k) for k in kys]).tocoo()
+    eng = object.__new__(S2.TorchDC2D)
+    dev, dt = torch.device("cpu"), torch.float64
+    eng.device, eng.dtype, eng.chunk = dev, dt, chunk
+    eng._sr, eng._P_inj, eng._primary = False, None, None
+    eng.kys = np.asarray(kys)
+    eng.nC, eng.nN, eng.nS, eng.nD = ops.nC, ops.nN, ops.nS, ops.nD
+    eng.nky, eng.nnzA = len(kys), ops.nnzA
+    eng.Lstack = torch.sparse_coo_tensor(
+        torch.tensor(np.vstack((L.row, L.col)), dtype=torch.int64),
+        torch.tensor(L.data), L.shape).coalesce()
+    eng.wq = torch.tensor(np.asarray(wq))
+    eng.q = torch.tensor(ops.q.toarray())
+    Pd = ops.Pd.tocoo()
+    eng.Pd = torch.sparse_coo_tensor(
+        torch.tensor(np.vstack((Pd.row, Pd.col)), dtype=torch.int64),
+        torch.tensor(Pd.data), Pd.shape).coalesce()
+    eng.sidx = torch.tensor(ops.sidx)
+    eng.iD = torch.arange(ops.nD)
+    eng._crow = torch.tensor(ops.crow, dtype=torch.int32)
+    eng._ccol = torch.tensor(ops.col, dtype=torch.int32)
+    eng._solvers = {}
+    eng._PdT = eng._PdTs = eng._PinjT = None
+    eng.solver = eng._solver_for(ops.nS)
+    return eng, sp.csr_matrix(L)
+
+
+def engine_3d(S3, S, ops):
+    L3 = ops.L3()
+    eng = object.__new__(S3.TorchDC3D)
+    eng.device, eng.dtype = torch.device("cpu"), torch.float64
+    eng._P_inj = eng._P_injt = None
+
+    def s2t(M):
+        M = sp.csr_matrix(M)
+        M.sort_indices()
+        return torch.sparse_csr_tensor(
+            torch.tensor(M.indptr, dtype=torch.int32),
+            torch.tensor(M.indices, dtype=torch.int32),
+            torch.tensor(M.data), size=M.shape)
+    eng.nC, eng.nN, eng.nS, eng.nD = ops.nC, ops.nN, ops.nS, ops.nD
+    eng.nnzA = ops.nnzA
+    eng.L3 = s2t(L3)
+    eng.L3t = s2t(L3.T)
+    eng.q = torch.tensor(ops.q.toarray())
+    eng.Pd = s2t(ops.Pd)
+    eng.sidx = torch.tensor(ops.sidx)
+    eng.iD = torch.arange(ops.nD)
+    eng.solver = S.make_solver(torch.tensor(ops.crow, dtype=torch.int32),
+                               torch.tensor(ops.col, dtype=torch.int32),
+                               ops.nN, ops.nS, device="cpu")
+    return eng, L3
+
+
+def run_engine(eng, m, dobs, w, v, two_d):
+    mt = torch.tensor(m, requires_grad=True)
+    phi = eng.misfit(mt, torch.tensor(dobs), torch.tensor(w))
+    phi.backward()
+    out = dict(phi=float(phi), grad=mt.grad.numpy().copy())
+    with torch.no_grad():
+        out["dpred"] = eng.dpred(torch.tensor(m)).numpy()
+    out["jtvec"] = eng.Jtvec(torch.tensor(m), torch.tensor(v)).numpy()
+    if two_d:
+        ch = max(1, eng.nS // 3)
+        out["jtvec_chunk"] = eng.Jtvec(torch.tensor(m), torch.tensor(v),
+                                       chunk=ch).numpy()
+        f, g = eng.misfit_and_grad(torch.tensor(m), torch.tensor(dobs),
+                                   torch.tensor(w), chunk=ch)
+        out["mag_phi"] = float(f)
+        out["mag_grad"] = g.numpy()
+        out["chunk"] = ch
+    return out
+
+
+def data_vectors(eng, m, seed):
+    rng = np.random.default_rng(seed)
+    with torch.no_grad():
+        d = eng.dpred(torch.tensor(m)).numpy()
+    dobs, w = syn.observed(d, rng, 0.05)
+    v = rng.standard_normal(d.size)
+    return dobs, w, v
+
+
+def checksums(ops):
+    return dict(ck_Ledge=float(np.abs(ops.L_edge.data).sum()),
+                ck_Lnode=float(np.abs(ops.L_node.data).sum()),
+                ck_bc=float(np.abs(ops.L_bc(0.1).data).sum()),
+                ck_q=float(np.abs(ops.q.data).sum()),
+                ck_Pd=float(np.abs(ops.Pd.data).sum()),
+                nnzA=ops.nnzA, nN=ops.nN, nC=ops.nC)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", required=True)
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    S, Q, S2, S3 = load_reference(a.reference)
+    out = a.out
+
+    np.savez_compressed(os.path.join(out, "solver_nx12.npz"),
+                        **solver_fixture(S, 12, 3, 1))
+    np.savez_compressed(os.path.join(out, "solver_nx40.npz"),
+                        **solver_fixture(S, 40, 5, 0))
+
+    qd = {}
+    for i, (lo, hi, n) in enumerate([(5.0, 120.0, 11), (5.0, 120.0, 7),
+                                     (2.0, 90.0, 12), (1.0, 60.0, 5)]):
+        p, w, info = Q.k0_quadrature(lo, hi, n)
+        qd[f"args{i}"] = np.array([lo, hi, n])
+        qd[f"pts{i}"] = p
+        qd[f"wts{i}"] = w
+        qd[f"err{i}"] = info["max_rel_err"]
+    np.savez_compressed(os.path.join(out, "quad.npz"), **qd)
+
+    for name, (mesh, survey, m), nky, store_ops in [
+            ("dc2d_tiny", syn.tiny_2d(), 7, True),
+            ("dc2d_suite", syn.suite_case("2d-tensor"), 11, False)]:
+        ops = nodal_operators(mesh, survey)
+        rmin, rmax = electrode_distance_range(survey)
+        kys, wq, _ = Q.k0_quadrature(rmin, rmax, nky)
+        eng, L = engine_2d(S2, ops, kys, wq)
+        dobs, w, v = data_vectors(eng, m, 21)
+        res = run_engine(eng, m, dobs, w, v, True)
+        rec = dict(m=m, dobs=dobs, w=w, v=v, kys=kys, wq=wq, **res,
+                   **checksums(ops))
+        if store_ops:
+            rec.update(L_indptr=L.indptr, L_indices=L.indices, L_data=L.data,
+                       crow=ops.crow, col=ops.col, Q=ops.q.toarray(),
+                       Pd_indptr=ops.Pd.indptr, Pd_indices=ops.Pd.indices,
+                       Pd_data=ops.Pd.data, sidx=ops.sidx)
+        np.savez_compressed(os.path.join(out, name + ".npz"), **rec)
+        print(name, "nN", ops.nN, "nD", ops.nD, "nky", len(kys))
+
+    for name, (mesh, survey, m), store_ops in [
+            ("dc3d_tiny", syn.tiny_3d(), True),
+            ("dc3d_suite", syn.suite_case("3d-tensor"), False)]:
+        ops = nodal_operators(mesh, survey)
+        eng, L3 = engine_3d(S3, S, ops)
+        dobs, w, v = data_vectors(eng, m, 22)
+        res = run_engine(eng, m, dobs, w, v, False)
+        rec = dict(m=m, dobs=dobs, w=w, v=v, **res, **checksums(ops))
+        if store_ops:
+            rec.update(L_indptr=L3.indptr, L_indices=L3.indices,
+                       L_data=L3.data, crow=ops.crow, col=ops.col,
+                       Q=ops.q.toarray(), Pd_indptr=ops.Pd.indptr,
+                       Pd_indices=ops.Pd.indices, Pd_data=ops.Pd.data,
+                       sidx=ops.sidx)
+        np.savez_compressed(os.path.join(out, name + ".npz"), **rec)
+        print(name, "nN", ops.nN, "nD", ops.nD)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,194 @@
+"""CPU replay of libdct's factor / solve launch schedules (test infrastructure).
+
+The schedules are exported through the C ABI (`dct_symbolic_get_schedule`)
+and every task is executed with numpy exactly as the corresponding kernel
+does it (same tiles, same reads and writes, same buffers A/B).  Each launch
+is replayed twice, in forward and in reversed task order, from the same
+starting state: since the kernels of one launch run in any order on the GPU,
+the two results must agree to round-off, which catches a task that reads
+what another task of the same launch writes.  Every index is bounds-checked.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PANEL = 64
+RHS_CHUNK = 32
+(SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, FWD, BWDGEMM, BWDSTEP) = range(8)
+
+
+class Struct:
+    def __init__(self, sym):
+        for name in ("perm", "iperm", "sn_first", "front_n", "front_off",
+                     "rows_ptr", "rows", "child_ptr", "child", "rel_ptr",
+                     "rel", "amap_ptr", "amap_e", "amap_pos", "sn_parent"):
+            setattr(self, name, sym.array(name))
+        self.nsuper = len(self.front_n)
+        self.front_total = int((self.front_n.astype(np.int64) ** 2).sum())
+
+    def ns(self, s):
+        return int(self.sn_first[s + 1] - self.sn_first[s])
+
+    def front(self, buf, s):
+        N = int(self.front_n[s])
+        off = int(self.front_off[s])
+        assert 0 <= off and off + N * N <= buf.size
+        return buf[off:off + N * N].reshape(N, N, order="F")
+
+
+def _chol_lower(D):
+    w = D.shape[0]
+    D = np.tril(D).copy()
+    for k in range(w):
+        piv = D[k, k]
+        assert piv > 0, "non-positive pivot in replay"
+        d = np.sqrt(piv)
+        D[k + 1:, k] /= d
+        D[k + 1:, k + 1:] -= np.tril(np.outer(D[k + 1:, k], D[k + 1:, k]))
+        D[k, k] = d
+    return D
+
+
+def _task_factor(S, kind, tk, fronts, vals, arg):
+    s, p, t0, t1 = (int(v) for v in tk)
+    N = int(S.front_n[s])
+    ns = S.ns(s)
+    F = S.front(fronts, s)
+    if kind == SMALL:
+        assert N <= arg
+        a0, a1 = S.amap_ptr[s], S.amap_ptr[s + 1]
+        pos = S.amap_pos[a0:a1]
+        assert pos.size == 0 or (pos.min() >= 0 and pos.max() < N * N)
+        flat = np.zeros(N * N)
+        flat[pos] = vals[S.amap_e[a0:a1]]
+        G = flat.reshape(N, N, order="F")
+        for ci in range(S.child_ptr[s], S.child_ptr[s + 1]):
+            c = int(S.child[ci])
+            nc, nsc = int(S.front_n[c]), S.ns(c)
+            U = S.front(fronts, c)[nsc:, nsc:]
+            rel = S.rel[S.rel_ptr[c]:S.rel_ptr[c + 1]]
+            assert rel.size == nc - nsc and (rel.size == 0 or rel.max() < N)
+            G[np.ix_(rel, rel)] += np.tril(U)
+        for k in range(ns):
+            piv = G[k, k]
+            assert piv > 0, f"non-positive pivot at supernode {s}"
+            d = np.sqrt(piv)
+            G[k + 1:, k] /= d
+            G[k + 1:, k + 1:] -= np.tril(np.outer(G[k + 1:, k], G[k + 1:, k]))
+            G[k, k] = d
+        F[:, :] = G
+    elif kind == LSCATTER:
+        a0, a1 = S.amap_ptr[s], S.amap_ptr[s + 1]
+        flat = fronts[int(S.front_off[s]):int(S.front_off[s]) + N * N]
+        flat[S.amap_pos[a0:a1]] = vals[S.amap_e[a0:a1]]
+    elif kind == LEXTEND:
+        c = t0
+        nc, nsc = int(S.front_n[c]), S.ns(c)
+        nbc = nc - nsc
+        U = S.front(fronts, c)
+        rel = S.rel[S.rel_ptr[c]:S.rel_ptr[c + 1]]
+        for j in range(t1, min(t1 + 8, nbc)):
+            i = np.arange(j, nbc)
+            F[rel[i], rel[j]] += U[nsc + i, nsc + j]
+    elif kind == LPANEL:
+        c0 = p * PANEL
+        w = min(PANEL, ns - c0)
+        assert w > 0 and t0 >= 1
+        D = _chol_lower(F[c0:c0 + w, c0:c0 + w])
+        r0 = c0 + w + (t0 - 1) * PANEL
+        nr = min(PANEL, N - r0)
+        assert nr > 0
+        X = F[r0:r0 + nr, c0:c0 + w]
+        F[r0:r0 + nr, c0:c0 + w] = np.linalg.solve(D, X.T).T
+    elif kind == LUPDATE:
+        c0 = p * PANEL
+        w = min(PANEL, ns - c0)
+        base = c0 + w
+        if t0 < 0:
+            F[c0:c0 + w, c0:c0 + w] = np.where(
+                np.tril(np.ones((w, w), bool)),
+                _chol_lower(F[c0:c0 + w, c0:c0 + w]), F[c0:c0 + w, c0:c0 + w])
+            return
+        ri, rj = base + t0 * PANEL, base + t1 * PANEL
+        assert ri < N and rj < N and t0 >= t1
+        ni, nj = min(PANEL, N - ri), min(PANEL, N - rj)
+        F[ri:ri + ni, rj:rj + nj] -= (F[ri:ri + ni, c0:c0 + w]
+                                      @ F[rj:rj + nj, c0:c0 + w].T)
+    else:
+        raise AssertionError(f"unexpected kind {kind}")
+
+
+def replay_factor(sym, S, vals, dtype=0):
+    tasks, launches = sym.schedule(dtype, 0)
+    fronts = np.zeros(S.front_total)
+    for kind, lv, first, count, arg in launches:
+        chunk = tasks[first:first + count]
+        snap = fronts.copy()
+        for tk in chunk:
+            _task_factor(S, kind, tk, fronts, vals, arg)
+        fwd_result = fronts.copy()
+        fronts[:] = snap
+        for tk in chunk[::-1]:
+            _task_factor(S, kind, tk, fronts, vals, arg)
+        scale = max(1.0, np.abs(fwd_result).max())
+        assert np.abs(fronts - fwd_result).max() <= 1e-9 * scale, \
+            f"launch kind {kind} level {lv}: result depends on task order"
+    return fronts
+
+
+def _task_solve(S, kind, tk, fronts, A, B):
+    s, p, t0, t1 = (int(v) for v in tk)
+    N = int(S.front_n[s])
+    ns = S.ns(s)
+    first = int(S.sn_first[s])
+    F = S.front(fronts, s)
+    c0 = p * PANEL
+    w = min(PANEL, ns - c0)
+    rows = S.rows[S.rows_ptr[s]:S.rows_ptr[s + 1]]
+    assert rows.size == N
+    if kind == FWD:
+        D = np.tril(F[c0:c0 + w, c0:c0 + w])
+        y = np.linalg.solve(D, A[first + c0:first + c0 + w])
+        if t0 == 0:
+            B[first + c0:first + c0 + w] = y
+            return
+        r0 = c0 + w + (t0 - 1) * PANEL
+        nr = min(PANEL, N - r0)
+        assert nr > 0
+        upd = F[r0:r0 + nr, c0:c0 + w] @ y
+        A[rows[r0:r0 + nr]] -= upd
+    elif kind == BWDGEMM:
+        xb = A[rows[ns:]]
+        B[first + c0:first + c0 + w] -= F[ns:, c0:c0 + w].T @ xb
+    elif kind == BWDSTEP:
+        D = np.tril(F[c0:c0 + w, c0:c0 + w])
+        x = np.linalg.solve(D.T, B[first + c0:first + c0 + w])
+        if t0 == p:
+            A[first + c0:first + c0 + w] = x
+            return
+        ci0 = t0 * PANEL
+        assert ci0 + PANEL <= c0
+        B[first + ci0:first + ci0 + PANEL] -= F[c0:c0 + w, ci0:ci0 + PANEL].T @ x
+    else:
+        raise AssertionError(f"unexpected kind {kind}")
+
+
+def replay_solve(sym, S, fronts, bp, dtype=0):
+    """bp: permuted rhs (n, k).  Returns the permuted solution."""
+    A = np.array(bp, dtype=float, copy=True)
+    B = np.zeros_like(A)
+    for which in (1, 2):
+        tasks, launches = sym.schedule(dtype, which)
+        for kind, lv, first, count, arg in launches:
+            chunk = tasks[first:first + count]
+            sa, sb = A.copy(), B.copy()
+            for tk in chunk:
+                _task_solve(S, kind, tk, fronts, A, B)
+            ra, rb = A.copy(), B.copy()
+            A[:], B[:] = sa, sb
+            for tk in chunk[::-1]:
+                _task_solve(S, kind, tk, fronts, A, B)
+            scale = max(1.0, np.abs(ra).max(), np.abs(rb).max())
+            assert max(np.abs(A - ra).max(), np.abs(B - rb).max()) <= 1e-9 * scale, \
+                f"solve launch kind {kind} level {lv}: depends on task order"
+    return A

@@ -1,0 +1,71 @@
+"""The CPU oracle against outputs of the reference itself (golden fixtures)."""
+import numpy as np
+import scipy.sparse as sp
+
+from conftest import golden
+from oracle import dc_oracle as O
+
+
+def _ops(g, three_d):
+    n = g["crow"].size - 1
+    L = sp.csr_matrix((g["L_data"], g["L_indices"], g["L_indptr"]))
+    Pd = sp.csr_matrix((g["Pd_data"], g["Pd_indices"], g["Pd_indptr"]),
+                       shape=(g["sidx"].size, n))
+    op = dict(crow=g["crow"], col=g["col"], nN=n, Q=g["Q"], Pd=Pd,
+              sidx=g["sidx"])
+    if three_d:
+        op["L3"] = L
+    else:
+        op["Lstack"] = L
+        op["wq"] = g["wq"]
+    return op
+
+
+def test_solver_forward_and_vjp_match_reference():
+    for name in ("solver_nx12", "solver_nx40"):
+        g = golden(name)
+        x, gv, gb = O.sparse_solve_vjp(g["crow"], g["col"], g["vals"], g["b"],
+                                       g["w"])
+        assert O.rel(x, g["x"]) < 1e-13
+        assert O.rel(gv, g["grad_vals"]) < 1e-12
+        assert O.rel(gb, g["grad_b"]) < 1e-12
+
+
+def test_dc2d_tiny_matches_reference():
+    g = golden("dc2d_tiny")
+    op = _ops(g, False)
+    m, dobs, w, v = g["m"], g["dobs"], g["w"], g["v"]
+    assert O.rel(O.dpred_2d(op, m), g["dpred"]) < 1e-12
+    phi, grad = O.misfit_grad_2d(op, m, dobs, w)
+    assert abs(phi - g["phi"]) <= 1e-12 * abs(g["phi"])
+    assert O.rel(grad, g["grad"]) < 1e-11
+    assert O.rel(O.jtvec_2d(op, m, v), g["jtvec"]) < 1e-11
+    # the reference's chunked products equal its whole-survey ones
+    assert O.rel(g["jtvec_chunk"], g["jtvec"]) < 1e-12
+    assert O.rel(g["mag_grad"], g["grad"]) < 1e-12
+
+
+def test_dc3d_tiny_matches_reference():
+    g = golden("dc3d_tiny")
+    op = _ops(g, True)
+    m, dobs, w, v = g["m"], g["dobs"], g["w"], g["v"]
+    assert O.rel(O.dpred_3d(op, m), g["dpred"]) < 1e-12
+    phi, grad = O.misfit_grad_3d(op, m, dobs, w)
+    assert abs(phi - g["phi"]) <= 1e-12 * abs(g["phi"])
+    assert O.rel(grad, g["grad"]) < 1e-11
+    assert O.rel(O.jtvec_3d(op, m, v), g["jtvec"]) < 1e-11
+
+
+def test_oracle_gradient_is_a_derivative():
+    """Central differences of the oracle's own misfit (no reference needed)."""
+    g = golden("dc2d_tiny")
+    op = _ops(g, False)
+    m, dobs, w = g["m"], g["dobs"], g["w"]
+    _, grad = O.misfit_grad_2d(op, m, dobs, w)
+    rng = np.random.default_rng(3)
+    u = rng.standard_normal(m.size)
+    u /= np.linalg.norm(u)
+    h = 1e-5
+    fd = (O.misfit_2d(op, m + h * u, dobs, w)
+          - O.misfit_2d(op, m - h * u, dobs, w)) / (2 * h)
+    assert abs(fd - grad @ u) <= 1e-6 * abs(fd)
