@@ -122,6 +122,17 @@ int dct_solve(dct_plan* plan, const void* d_b, int32_t io_dtype,
 int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
                        int32_t k, double* d_xp, void* stream);
 
+/* Per-launch-kind timing with CUDA events on the launch stream (off by
+ * default).  While enabled, every factor/solve launch is bracketed by events;
+ * dct_plan_profile_get synchronises and returns, for one launch kind
+ * (0 small fronts, 1 large scatter, 2 extend-add, 3 panel, 4 trailing
+ * update, 5 forward step, 6 backward gemm, 7 backward step), the summed
+ * device milliseconds, the launch count and the algorithmic flops and bytes
+ * of those launches; reset clears the counters. */
+int dct_plan_profile(dct_plan* plan, int32_t enable, int32_t reset);
+int dct_plan_profile_get(dct_plan* plan, int32_t kind, double* ms,
+                         int64_t* launches, double* flops, double* bytes);
+
 /* Reads the device status words (synchronises the stream): the first error
  * code raised by a kernel since the last call, the supernode where it was
  * raised (or -1) and the last refinement residual ratio max|b-Ax|/max|b|. */

@@ -107,11 +107,12 @@ def dpred_2d(op, m, return_fields=False):
     return d
 
 
-def _adjoint_2d(op, m, g_data):
+def _adjoint_2d(op, m, g_data, fields=None):
     """dL/dm for dL/dd = g_data through the 2.5-D chain (the autograd path of
-    simulation2d.py:378-396 with solver.py:261-281 and the Lstack vjp)."""
+    simulation2d.py:378-396 with solver.py:261-281 and the Lstack vjp).
+    `fields` = dpred_2d(..., return_fields=True) reuses that factorization."""
     nky = len(op["wq"])
-    d, VALS, slv, U = dpred_2d(op, m, return_fields=True)
+    d, VALS, slv, U = fields or dpred_2d(op, m, return_fields=True)
     nS = op["Q"].shape[1]
     nN = op["nN"]
     # dL/dUbar[:, s] = Pd^T (g restricted to source s)
@@ -135,9 +136,10 @@ def misfit_2d(op, m, dobs, w):
 
 
 def misfit_grad_2d(op, m, dobs, w):
-    d = dpred_2d(op, m)
-    r = w * (d - dobs)
-    _, g = _adjoint_2d(op, m, 2.0 * w * r)
+    """(phi, dphi/dm) with one factorization, as misfit().backward() does."""
+    fields = dpred_2d(op, m, return_fields=True)
+    r = w * (fields[0] - dobs)
+    _, g = _adjoint_2d(op, m, 2.0 * w * r, fields)
     return float((r ** 2).sum()), g
 
 
@@ -160,8 +162,8 @@ def dpred_3d(op, m, return_fields=False):
     return d
 
 
-def _adjoint_3d(op, m, g_data):
-    d, slv, U = dpred_3d(op, m, return_fields=True)
+def _adjoint_3d(op, m, g_data, fields=None):
+    d, slv, U = fields or dpred_3d(op, m, return_fields=True)
     G = np.zeros((op["Pd"].shape[0], op["Q"].shape[1]))
     G[np.arange(G.shape[0]), op["sidx"]] = g_data
     Y = slv.solve(op["Pd"].T @ G)[0]
@@ -171,9 +173,10 @@ def _adjoint_3d(op, m, g_data):
 
 
 def misfit_grad_3d(op, m, dobs, w):
-    d = dpred_3d(op, m)
-    r = w * (d - dobs)
-    _, g = _adjoint_3d(op, m, 2.0 * w * r)
+    """(phi, dphi/dm) with one factorization (simulation3d.py:224-227 + backward)."""
+    fields = dpred_3d(op, m, return_fields=True)
+    r = w * (fields[0] - dobs)
+    _, g = _adjoint_3d(op, m, 2.0 * w * r, fields)
     return float((r ** 2).sum()), g
 
 

@@ -69,6 +69,10 @@ _SIGS = {
     "dct_factorize": (C.c_int, [_p, _p, _i32, _i64, _p]),
     "dct_solve": (C.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
     "dct_solve_permuted": (C.c_int, [_p, _p, _i32, _i32, _p, _p]),
+    "dct_plan_profile": (C.c_int, [_p, _i32, _i32]),
+    "dct_plan_profile_get": (C.c_int, [_p, _i32, C.POINTER(C.c_double), _pi64,
+                                       C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]),
     "dct_check_status": (C.c_int, [_p, _p, _pi32, _pi32,
                                    C.POINTER(C.c_double)]),
     "dct_sigma_values": (C.c_int, [_i64, _p, _p, _p, _i64, _p, _p, _p, _p]),
@@ -217,6 +221,25 @@ class Plan:
     def solve_permuted(self, d_bp, b_batched, k, d_xp, stream):
         check(lib().dct_solve_permuted(self._h, d_bp, int(b_batched), int(k),
                                        d_xp, stream), "dct_solve_permuted")
+
+    KINDS = ("small_front", "large_scatter", "extend_add", "panel_trsm",
+             "trailing_update", "fwd_step", "bwd_gemm", "bwd_step")
+
+    def profile(self, enable, reset=True):
+        check(lib().dct_plan_profile(self._h, int(bool(enable)), int(reset)),
+              "dct_plan_profile")
+
+    def profile_read(self):
+        """{kind: (ms, launches, flops, bytes)} accumulated while enabled."""
+        out = {}
+        for k, name in enumerate(self.KINDS):
+            ms, n = C.c_double(0), C.c_int64(0)
+            fl, by = C.c_double(0), C.c_double(0)
+            check(lib().dct_plan_profile_get(self._h, k, C.byref(ms), C.byref(n),
+                                             C.byref(fl), C.byref(by)),
+                  "dct_plan_profile_get")
+            out[name] = (ms.value, n.value, fl.value, by.value)
+        return out
 
     def status(self, stream):
         code, where, res = C.c_int32(0), C.c_int32(0), C.c_double(0.0)

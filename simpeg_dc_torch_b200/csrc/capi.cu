@@ -59,6 +59,118 @@ int alloc(dct_plan* P, size_t bytes, void** out, const char* what) {
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 // ---- schedules ------------------------------------------------------------
+// Algorithmic work of each launch (see dct::Schedule).  es = element size.
+void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es) {
+  sc->flops.assign(sc->launches.size(), 0.0);
+  sc->bytes.assign(sc->launches.size(), 0.0);
+  sc->bytes_rhs.assign(sc->launches.size(), 0.0);
+  for (size_t li = 0; li < sc->launches.size(); ++li) {
+    const Launch& l = sc->launches[li];
+    double f = 0, b = 0;
+    for (int64_t q = l.first; q < l.first + l.count; ++q) {
+      const PanelTask& t = sc->tasks[q];
+      const int s = t.s, N = S.front_n[s], ns = S.ns(s);
+      const int c0 = t.p * dct::kPanel, w = std::min(dct::kPanel, ns - c0);
+      switch (l.kind) {
+        case dct::kSmallFront: {
+          for (int k = 0; k < ns; ++k) {
+            double m = N - k - 1;
+            f += 1 + m + m * (m + 1);
+          }
+          double upd = 0;
+          for (int ci = S.child_ptr[s]; ci < S.child_ptr[s + 1]; ++ci) {
+            double nbc = S.nb(S.child[ci]);
+            upd += nbc * (nbc + 1) / 2;
+          }
+          double nent = double(S.amap_ptr[s + 1] - S.amap_ptr[s]);
+          b += es * (double(N) * N + upd) + nent * (es + 8);
+          break;
+        }
+        case dct::kLargeScatter:
+          b += double(S.amap_ptr[s + 1] - S.amap_ptr[s]) * (2 * es + 8);
+          break;
+        case dct::kLargeExtendAdd: {
+          const int nbc = S.nb(t.t0);
+          double cols = std::min(8, nbc - t.t1), el = 0;
+          for (int j = t.t1; j < t.t1 + cols; ++j) el += nbc - j;
+          f += el;
+          b += el * 3 * es;
+          break;
+        }
+        case dct::kLargePanel: {
+          const int r0 = c0 + w + (t.t0 - 1) * dct::kPanel;
+          const double nr = std::min(dct::kPanel, N - r0);
+          f += nr * w * w;
+          b += es * (2 * nr * w + w * w / 2.0);
+          break;
+        }
+        case dct::kLargeUpdate: {
+          if (t.t0 < 0) {
+            f += double(w) * w * w / 3.0;
+            b += es * w * w;
+            break;
+          }
+          const int base = c0 + w;
+          const double ni = std::min(dct::kPanel, N - (base + t.t0 * dct::kPanel));
+          const double nj = std::min(dct::kPanel, N - (base + t.t1 * dct::kPanel));
+          f += 2 * ni * nj * w;
+          b += es * ((ni + nj) * w + 2 * ni * nj);
+          break;
+        }
+        default:
+          break;
+      }
+    }
+    sc->flops[li] = f;
+    sc->bytes[li] = b;
+  }
+}
+
+void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
+  sc->flops.assign(sc->launches.size(), 0.0);
+  sc->bytes.assign(sc->launches.size(), 0.0);
+  sc->bytes_rhs.assign(sc->launches.size(), 0.0);
+  for (size_t li = 0; li < sc->launches.size(); ++li) {
+    const Launch& l = sc->launches[li];
+    double f = 0, bf = 0, br = 0;
+    for (int64_t q = l.first; q < l.first + l.count; ++q) {
+      const PanelTask& t = sc->tasks[q];
+      const int s = t.s, N = S.front_n[s], ns = S.ns(s);
+      const int c0 = t.p * dct::kPanel, w = std::min(dct::kPanel, ns - c0);
+      if (l.kind == dct::kFwdStep) {
+        if (t.t0 == 0) {
+          f += double(w) * w;
+          bf += es * w * (w + 1) / 2.0;
+          br += es * 2.0 * w;
+        } else {
+          const int r0 = c0 + w + (t.t0 - 1) * dct::kPanel;
+          const double nr = std::min(dct::kPanel, N - r0);
+          f += 2 * nr * w;
+          bf += es * nr * w;
+          br += es * 2 * nr;
+        }
+      } else if (l.kind == dct::kBwdGemm) {
+        const double nbd = N - ns;
+        f += 2 * nbd * w;
+        bf += es * nbd * w;
+        br += es * (nbd + 2.0 * w);
+      } else if (l.kind == dct::kBwdStep) {
+        f += double(w) * w;
+        bf += es * w * (w + 1) / 2.0;
+        br += es * 2.0 * w;
+        if (t.t0 != t.p) {
+          f += 2.0 * w * dct::kPanel;
+          bf += es * w * dct::kPanel;
+          br += es * 2.0 * dct::kPanel;
+        }
+      }
+    }
+    sc->flops[li] = f;
+    sc->bytes[li] = bf;
+    sc->bytes_rhs[li] = br;
+  }
+}
+
 void build_factor_schedule(const dct::Symbolic& S, int small_max,
                            dct::Schedule* out) {
   auto& T = out->tasks;
@@ -198,6 +310,53 @@ int set_device(int device) {
 }  // namespace
 
 void dct::set_last_error(const char* msg) { g_err = msg; }
+
+cudaError_t dct::Profiler::begin(int kind, double flops, double bytes,
+                                 cudaStream_t st) {
+  if (!on) return cudaSuccess;
+  Rec r{kind, nullptr, nullptr, flops, bytes};
+  for (cudaEvent_t* ev : {&r.a, &r.b}) {
+    if (!pool.empty()) {
+      *ev = pool.back();
+      pool.pop_back();
+    } else {
+      cudaError_t e = cudaEventCreate(ev);
+      if (e != cudaSuccess) return e;
+    }
+  }
+  recs.push_back(r);
+  return cudaEventRecord(r.a, st);
+}
+
+cudaError_t dct::Profiler::end(cudaStream_t st) {
+  if (!on || recs.empty()) return cudaSuccess;
+  return cudaEventRecord(recs.back().b, st);
+}
+
+cudaError_t dct::Profiler::collect() {
+  for (Rec& r : recs) {
+    cudaError_t e = cudaEventSynchronize(r.b);
+    if (e != cudaSuccess) return e;
+    float t = 0.f;
+    e = cudaEventElapsedTime(&t, r.a, r.b);
+    if (e != cudaSuccess) return e;
+    ms[r.kind] += t;
+    fl[r.kind] += r.flops;
+    by[r.kind] += r.bytes;
+    n[r.kind] += 1;
+    pool.push_back(r.a);
+    pool.push_back(r.b);
+  }
+  recs.clear();
+  return cudaSuccess;
+}
+
+void dct::Profiler::reset() {
+  for (int k = 0; k < 8; ++k) {
+    ms[k] = fl[k] = by[k] = 0.0;
+    n[k] = 0;
+  }
+}
 
 extern "C" {
 
@@ -370,6 +529,9 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
   build_factor_schedule(S, small_max, &P->fact);
   build_solve_schedules(S, &P->fwd, &P->bwd);
+  account_factor(S, &P->fact, double(esize(dtype)));
+  account_solve(S, &P->fwd, double(esize(dtype)));
+  account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||
       (rc = upload_schedule(P, &P->bwd)))
     return bail(rc);
@@ -512,6 +674,29 @@ int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
   DCT_CUDA(dct::launch_perm_out_any(P->x64, DCT_F64, P->ds.perm, n, k, P->nbatch,
                                     d_x, io_dtype, st),
            "permute solution");
+  return DCT_OK;
+}
+
+int dct_plan_profile(dct_plan* P, int32_t enable, int32_t reset) {
+  if (!P) return fail(DCT_ERR_ARG, "null plan");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  DCT_CUDA(P->prof.collect(), "profile collect");
+  if (reset) P->prof.reset();
+  P->prof.on = enable != 0;
+  return DCT_OK;
+}
+
+int dct_plan_profile_get(dct_plan* P, int32_t kind, double* ms, int64_t* launches,
+                         double* flops, double* bytes) {
+  if (!P || kind < 0 || kind > 7) return fail(DCT_ERR_ARG, "bad arguments");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  DCT_CUDA(P->prof.collect(), "profile collect");
+  if (ms) *ms = P->prof.ms[kind];
+  if (launches) *launches = P->prof.n[kind];
+  if (flops) *flops = P->prof.fl[kind];
+  if (bytes) *bytes = P->prof.by[kind];
   return DCT_OK;
 }
 

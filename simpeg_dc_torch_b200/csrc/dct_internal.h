@@ -60,6 +60,30 @@ struct Schedule {
   std::vector<PanelTask> tasks;    // host copy
   PanelTask* d_tasks = nullptr;    // device copy
   std::vector<Launch> launches;
+  // per launch, algorithmic work: factor launches give absolute flops and
+  // bytes; solve launches give flops per right-hand side, bytes that do not
+  // depend on k (factor reads) and bytes per right-hand side
+  std::vector<double> flops;
+  std::vector<double> bytes;
+  std::vector<double> bytes_rhs;
+};
+
+// Optional per-launch event timing (dct_plan_profile).
+struct Profiler {
+  bool on = false;
+  struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+    double flops, bytes;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  double ms[8] = {0}, fl[8] = {0}, by[8] = {0};
+  int64_t n[8] = {0};
+  cudaError_t begin(int kind, double flops, double bytes, cudaStream_t st);
+  cudaError_t end(cudaStream_t st);
+  cudaError_t collect();
+  void reset();
 };
 
 }  // namespace dct
@@ -88,6 +112,7 @@ struct dct_plan {
   int factored = 0;
   int64_t stamp = 0;
   int ir_iters = 2;                // refinement iterations of f32 plans
+  dct::Profiler prof;
 };
 
 struct dct_symbolic {

@@ -326,8 +326,11 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                              static_cast<int>(update_smem));
   if (e != cudaSuccess) return e;
   const PanelTask* tasks = P->fact.d_tasks;
-  for (const Launch& L : P->fact.launches) {
+  for (size_t li = 0; li < P->fact.launches.size(); ++li) {
+    const Launch& L = P->fact.launches[li];
     if (L.count <= 0) continue;
+    e = P->prof.begin(L.kind, P->fact.flops[li] * nb, P->fact.bytes[li] * nb, st);
+    if (e != cudaSuccess) return e;
     // grid.x is limited to 2^31-1, far above any task count here
     dim3 grid(static_cast<unsigned>(L.count), nb);
     const PanelTask* t = tasks + L.first;
@@ -359,6 +362,8 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
         return cudaErrorInvalidValue;
     }
     e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = P->prof.end(st);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

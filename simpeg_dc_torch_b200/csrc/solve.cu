@@ -332,16 +332,28 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
                              static_cast<int>(gemm_smem));
   if (e != cudaSuccess) return e;
   const T* fronts = static_cast<const T*>(P->fronts);
-  for (const Launch& L : P->fwd.launches) {
+  const double nb = P->nbatch;
+  for (size_t li = 0; li < P->fwd.launches.size(); ++li) {
+    const Launch& L = P->fwd.launches[li];
     if (L.count <= 0) continue;
+    if ((e = P->prof.begin(L.kind, P->fwd.flops[li] * k * nb,
+                           (P->fwd.bytes[li] + P->fwd.bytes_rhs[li] * k) * nb,
+                           st)) != cudaSuccess)
+      return e;
     dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
     k_fwd_step<T><<<grid, kThreads, step_smem, st>>>(
         P->ds, P->fwd.d_tasks + L.first, fronts, P->front_stride, bufA, bufB, n,
         k, nchunk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = P->prof.end(st)) != cudaSuccess) return e;
   }
-  for (const Launch& L : P->bwd.launches) {
+  for (size_t li = 0; li < P->bwd.launches.size(); ++li) {
+    const Launch& L = P->bwd.launches[li];
     if (L.count <= 0) continue;
+    if ((e = P->prof.begin(L.kind, P->bwd.flops[li] * k * nb,
+                           (P->bwd.bytes[li] + P->bwd.bytes_rhs[li] * k) * nb,
+                           st)) != cudaSuccess)
+      return e;
     dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
     if (L.kind == kBwdGemm)
       k_bwd_gemm<T><<<grid, kThreads, gemm_smem, st>>>(
@@ -352,6 +364,7 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
           P->ds, P->bwd.d_tasks + L.first, fronts, P->front_stride, bufA, bufB,
           n, k, nchunk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = P->prof.end(st)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

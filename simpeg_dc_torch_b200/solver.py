@@ -87,8 +87,9 @@ class _PlanSolver:
         with torch.cuda.device(self.device):
             self._plan = nat.Plan(self._sym, self.nbatch, self.n_rhs,
                                   self._code, self.device.index)
-        if refine is not None:
-            self._plan.set_refinement(int(refine))
+        # refinement iterations of float32 plans (the library default is 2)
+        self.refine = 2 if refine is None else int(refine)
+        self._plan.set_refinement(self.refine)
         self.stamp = 0
 
     # ---- introspection
