@@ -196,6 +196,23 @@ int dct_gather_contract_plain(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
                               int32_t dtype, const void* d_Y, const void* d_X,
                               void* d_gv, void* stream);
 
+/* ---- allocation-free small solve -------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (work inside a stream being captured into a CUDA graph, hosts whose
+ * framework owns all device memory, loops that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree): factors one SPD system given by
+ * its CSR pattern and values (n <= 512; the lower triangle is read) and
+ * solves k <= 64 right-hand sides, b and x row-major (n, k) float64 on the
+ * current device.  Its only scratch is a fixed 2 MiB array in the library
+ * (held by every GPU that loads the library until exit); sizes beyond the
+ * limits return DCT_ERR_ARG.  The first call on a device looks up that
+ * array's address and must come before any stream capture.  Calls share the
+ * array, so calls that may overlap on the GPU race and must be ordered. */
+int dct_solve_small_noalloc(int32_t n, const int32_t* d_crow,
+                            const int32_t* d_col, const double* d_vals,
+                            const double* d_b, int32_t k, double* d_x,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif

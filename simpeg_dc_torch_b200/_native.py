@@ -85,6 +85,7 @@ _SIGS = {
                                       _p, _p, _p, _p]),
     "dct_gather_contract_plain": (C.c_int, [_i32, _i64, _i64, _i32, _p, _p,
                                             _i32, _p, _p, _p, _p]),
+    "dct_solve_small_noalloc": (C.c_int, [_i32, _p, _p, _p, _p, _i32, _p, _p]),
 }
 
 
