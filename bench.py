@@ -220,7 +220,8 @@ def count_launches(eng):
     solve = (per[1] + per[2]) * (1 + ir) + (1 if code == 0 else 1 + (1 + ir) + ir)
     # sigma + values, source scatter, projection, adjoint scatter, gather,
     # values vjp; factor; two solves
-    return per[0] + 2 * solve + 6
+    # + the panel-inverse launch of the factorization
+    return per[0] + 1 + 2 * solve + 6
 
 
 def main():

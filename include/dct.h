@@ -37,7 +37,8 @@ enum {
   DCT_ERR_IR_NOT_CONVERGED = 5, /* refinement residual above tolerance */
   DCT_ERR_BAD_PATTERN = 6,      /* pattern rejected by the analysis */
   DCT_ERR_NOT_FACTORED = 7,     /* solve before factorize */
-  DCT_ERR_NO_DEVICE = 8         /* no usable CUDA device */
+  DCT_ERR_NO_DEVICE = 8,        /* no usable CUDA device */
+  DCT_ERR_DEVICE_TIMEOUT = 9    /* a bounded on-device wait gave up */
 };
 
 typedef struct dct_symbolic dct_symbolic;
@@ -78,7 +79,8 @@ int dct_symbolic_get_array(const dct_symbolic* sym, const char* name,
                            int64_t* size_bytes);
 
 /* Host-side copy of the launch schedule a plan of this dtype would run
- * (which: 0 factorization, 1 forward, 2 backward substitution), for
+ * (which: 0 factorization, 1 forward, 2 backward substitution, 3 panel
+ * inverses), for
  * inspection and CPU-side replay in tests.  tasks: 4 int32 per task
  * (supernode, panel, t0, t1); launches: 5 int64 per launch (kind, level,
  * first task, task count, arg).  With null outputs only the counts are set. */
@@ -126,7 +128,9 @@ int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
  * default).  While enabled, every factor/solve launch is bracketed by events;
  * dct_plan_profile_get synchronises and returns, for one launch kind
  * (0 small fronts, 1 large scatter, 2 extend-add, 3 panel, 4 trailing
- * update, 5 forward step, 6 backward gemm, 7 backward step), the summed
+ * update, 5 forward step, 6 backward gemm, 7 backward step, 8 forward of
+ * single-panel supernodes, 9 backward of single-panel supernodes, 10 panel
+ * inverses, 11 forward row tiles on tensor cores), the summed
  * device milliseconds, the launch count and the algorithmic flops and bytes
  * of those launches; reset clears the counters. */
 int dct_plan_profile(dct_plan* plan, int32_t enable, int32_t reset);

@@ -47,7 +47,7 @@ class FusedPath:
     """
 
     def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
-                 coords=None, refine=None, n_rhs=None):
+                 coords=None, refine=None, n_rhs=None, refine_fields=None):
         self.device = device
         nN = crow.size - 1
         self.nN, self.nnzA = nN, col.size
@@ -62,6 +62,13 @@ class FusedPath:
                                      refine=refine)
         plan = self.solver.plan
         self._plan = plan
+        # float32 plans: refinement iterations of the forward and of the
+        # adjoint fields.  One iteration brings the data to ~1e-8, but the
+        # gradient contracts both fields at every node and needs two each
+        # (measured on the 3-D workload: 3e-3 with one, 3e-6 with two).
+        self.refine_adj = self.solver.refine
+        self.refine_fields = (self.refine_adj if refine_fields is None
+                              else int(refine_fields))
         self._iperm_ptr = plan.d_iperm
         perm = self.solver._sym.array("perm")
         iperm = np.empty_like(perm)
@@ -146,6 +153,7 @@ class FusedPath:
 
     def fields(self):
         """U = A^{-1} Q, permuted (nbatch, nN, nS)."""
+        self._plan.set_refinement(self.refine_fields)
         return self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
 
     def project(self, U):
@@ -177,6 +185,7 @@ class FusedPath:
         """dL/dm_full for dL/dd = gd on the current factorization."""
         g = gd.detach().to(self.device, torch.float64).contiguous()
         R = self._scatter(self._adj, g, self.nS)
+        self._plan.set_refinement(self.refine_adj)
         Y = self._solve_perm(R, self.nS)
         gv = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
                          device=self.device)

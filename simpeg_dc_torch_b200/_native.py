@@ -22,6 +22,7 @@ STATUS = {
     4: "non-positive pivot (matrix not SPD)",
     5: "iterative refinement did not converge", 6: "pattern rejected",
     7: "solve before factorize", 8: "no CUDA device",
+    9: "a bounded device wait timed out",
 }
 
 
@@ -224,7 +225,8 @@ class Plan:
                                        d_xp, stream), "dct_solve_permuted")
 
     KINDS = ("small_front", "large_scatter", "extend_add", "panel_trsm",
-             "trailing_update", "fwd_step", "bwd_gemm", "bwd_step")
+             "trailing_update", "fwd_step", "bwd_gemm", "bwd_step",
+             "fwd_small", "bwd_small", "panel_inverse", "fwd_tc")
 
     def profile(self, enable, reset=True):
         check(lib().dct_plan_profile(self._h, int(bool(enable)), int(reset)),

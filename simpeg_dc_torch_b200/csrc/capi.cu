@@ -60,7 +60,8 @@ int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 // ---- schedules ------------------------------------------------------------
 // Algorithmic work of each launch (see dct::Schedule).  es = element size.
-void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es) {
+void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
+                    int utile) {
   sc->flops.assign(sc->launches.size(), 0.0);
   sc->bytes.assign(sc->launches.size(), 0.0);
   sc->bytes_rhs.assign(sc->launches.size(), 0.0);
@@ -106,15 +107,19 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es) {
         }
         case dct::kLargeUpdate: {
           if (t.t0 < 0) {
-            f += double(w) * w * w / 3.0;
-            b += es * w * w;
+            f += 2.0 * double(w) * w * w / 3.0;
+            b += es * 2.0 * w * w;
             break;
           }
           const int base = c0 + w;
-          const double ni = std::min(dct::kPanel, N - (base + t.t0 * dct::kPanel));
-          const double nj = std::min(dct::kPanel, N - (base + t.t1 * dct::kPanel));
+          const double ni = std::min(utile, N - (base + t.t0 * utile));
+          const double nj = std::min(utile, N - (base + t.t1 * utile));
           f += 2 * ni * nj * w;
           b += es * ((ni + nj) * w + 2 * ni * nj);
+          if (t.t0 == 0 && t.t1 == 0 && base < ns) {
+            const double w2 = std::min(dct::kPanel, ns - base);
+            f += 2.0 * w2 * w2 * w2 / 3.0;
+          }
           break;
         }
         default:
@@ -137,20 +142,34 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
       const PanelTask& t = sc->tasks[q];
       const int s = t.s, N = S.front_n[s], ns = S.ns(s);
       const int c0 = t.p * dct::kPanel, w = std::min(dct::kPanel, ns - c0);
-      if (l.kind == dct::kFwdStep) {
+      const double nbd = N - ns;
+      if (l.kind == dct::kFwdSmall) {
+        f += double(w) * w + 2 * nbd * w;
+        bf += es * (w * (w + 1) / 2.0 + nbd * w);
+        br += es * (2.0 * w + 2 * nbd);
+      } else if (l.kind == dct::kBwdSmall) {
+        f += double(w) * w + 2 * nbd * w;
+        bf += es * (w * (w + 1) / 2.0 + nbd * w);
+        br += es * (2.0 * w + nbd);
+      } else if (l.kind == dct::kFwdTc) {
+        const int r0 = c0 + w + t.t0 * 128;
+        const double nr = std::min(128, N - r0);
+        f += 2 * nr * w;
+        bf += es * nr * w;
+        br += es * (2 * nr + w);
+      } else if (l.kind == dct::kFwdStep) {
         if (t.t0 == 0) {
           f += double(w) * w;
           bf += es * w * (w + 1) / 2.0;
           br += es * 2.0 * w;
         } else {
           const int r0 = c0 + w + (t.t0 - 1) * dct::kPanel;
-          const double nr = std::min(dct::kPanel, N - r0);
+          const double nr = std::min(t.t1 * dct::kPanel + c0 + w, N) - r0;
           f += 2 * nr * w;
           bf += es * nr * w;
           br += es * 2 * nr;
         }
       } else if (l.kind == dct::kBwdGemm) {
-        const double nbd = N - ns;
         f += 2 * nbd * w;
         bf += es * nbd * w;
         br += es * (nbd + 2.0 * w);
@@ -171,7 +190,11 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
   }
 }
 
-void build_factor_schedule(const dct::Symbolic& S, int small_max,
+// trailing-update tile: 64 for float64 (CUDA cores), 128 for float32
+// (tcgen05 tensor-core tiles, M = N = 128)
+int update_tile(int dtype) { return dtype == DCT_F64 ? dct::kUpdateTile : 128; }
+
+void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile,
                            dct::Schedule* out) {
   auto& T = out->tasks;
   auto& L = out->launches;
@@ -210,6 +233,12 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max,
       l.count = int64_t(T.size()) - l.first;
       L.push_back(l);
     }
+    {
+      // the first panel's diagonal block of every large front
+      Launch ld{dct::kLargeUpdate, lv, int64_t(T.size()), int64_t(large.size()), 0};
+      for (int s : large) T.push_back({s, 0, -1, 0});
+      L.push_back(ld);
+    }
     int max_panels = 0;
     for (int s : large) max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
     for (int p = 0; p < max_panels; ++p) {
@@ -230,8 +259,7 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max,
         int c0 = p * dct::kPanel;
         if (c0 >= ns) continue;
         int w = std::min(dct::kPanel, ns - c0);
-        int nt = ceil_div(N - c0 - w, dct::kPanel);
-        T.push_back({s, p, -1, 0});
+        int nt = ceil_div(N - c0 - w, utile);
         for (int i = 0; i < nt; ++i)
           for (int j = 0; j <= i; ++j) T.push_back({s, p, i, j});
       }
@@ -241,50 +269,108 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max,
   }
 }
 
-void build_solve_schedules(const dct::Symbolic& S, dct::Schedule* fwd,
+void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
                            dct::Schedule* bwd) {
+  // float32 plans apply the row tiles below a panel on the tensor cores
+  // (128-row tiles, kFwdTc) after a launch that forms y_p (k_fwd_step, t0 = 0)
+  const bool tc = dtype == DCT_F32;
+  auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel; };
   for (int lv = 0; lv < S.nlevels; ++lv) {
+    Launch ls{dct::kFwdSmall, lv, int64_t(fwd->tasks.size()), 0, 0};
     int max_panels = 0;
-    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q)
-      max_panels = std::max(max_panels, ceil_div(S.ns(S.level_sn[q]), dct::kPanel));
+    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+      int s = S.level_sn[q];
+      if (is_small(s)) fwd->tasks.push_back({s, 0, 0, 0});
+      else max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
+    }
+    ls.count = int64_t(fwd->tasks.size()) - ls.first;
+    if (ls.count) fwd->launches.push_back(ls);
     for (int p = 0; p < max_panels; ++p) {
       Launch l{dct::kFwdStep, lv, int64_t(fwd->tasks.size()), 0, p};
       for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
         int s = S.level_sn[q];
+        if (is_small(s)) continue;
         int ns = S.ns(s), N = S.front_n[s];
         int c0 = p * dct::kPanel;
         if (c0 >= ns) continue;
         int w = std::min(dct::kPanel, ns - c0);
         int nt = ceil_div(N - c0 - w, dct::kPanel);
-        for (int t = 0; t <= nt; ++t) fwd->tasks.push_back({s, p, t, 0});
+        fwd->tasks.push_back({s, p, 0, 0});
+        if (!tc)
+          for (int t = 0; t < nt; t += dct::kRowGroup)
+            fwd->tasks.push_back({s, p, t + 1, std::min(nt, t + dct::kRowGroup)});
       }
       l.count = int64_t(fwd->tasks.size()) - l.first;
       fwd->launches.push_back(l);
+      if (tc) {
+        Launch lt{dct::kFwdTc, lv, int64_t(fwd->tasks.size()), 0, p};
+        for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+          int s = S.level_sn[q];
+          if (is_small(s)) continue;
+          int ns = S.ns(s), N = S.front_n[s];
+          int c0 = p * dct::kPanel;
+          if (c0 >= ns) continue;
+          int w = std::min(dct::kPanel, ns - c0);
+          int nt = ceil_div(N - c0 - w, 128);
+          for (int t = 0; t < nt; ++t) fwd->tasks.push_back({s, p, t, 0});
+        }
+        lt.count = int64_t(fwd->tasks.size()) - lt.first;
+        if (lt.count) fwd->launches.push_back(lt);
+      }
     }
   }
   for (int lv = S.nlevels - 1; lv >= 0; --lv) {
-    Launch lg{dct::kBwdGemm, lv, int64_t(bwd->tasks.size()), 0, 0};
+    Launch ls{dct::kBwdSmall, lv, int64_t(bwd->tasks.size()), 0, 0};
     int max_panels = 0;
     for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
       int s = S.level_sn[q];
+      if (is_small(s)) bwd->tasks.push_back({s, 0, 0, 0});
+      else max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
+    }
+    ls.count = int64_t(bwd->tasks.size()) - ls.first;
+    if (ls.count) bwd->launches.push_back(ls);
+    if (max_panels == 0) continue;
+    Launch lg{dct::kBwdGemm, lv, int64_t(bwd->tasks.size()), 0, 0};
+    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
+      int s = S.level_sn[q];
+      if (is_small(s) || S.nb(s) == 0) continue;
       int np = ceil_div(S.ns(s), dct::kPanel);
-      max_panels = std::max(max_panels, np);
-      if (S.nb(s) == 0) continue;
       for (int p = 0; p < np; ++p) bwd->tasks.push_back({s, p, 0, 0});
     }
     lg.count = int64_t(bwd->tasks.size()) - lg.first;
-    bwd->launches.push_back(lg);
+    if (lg.count) bwd->launches.push_back(lg);
     for (int p = max_panels - 1; p >= 0; --p) {
       Launch l{dct::kBwdStep, lv, int64_t(bwd->tasks.size()), 0, p};
       for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
         int s = S.level_sn[q];
-        if (p * dct::kPanel >= S.ns(s)) continue;
+        if (is_small(s) || p * dct::kPanel >= S.ns(s)) continue;
         for (int i = 0; i <= p; ++i) bwd->tasks.push_back({s, p, i, 0});
       }
       l.count = int64_t(bwd->tasks.size()) - l.first;
       bwd->launches.push_back(l);
     }
   }
+}
+
+// diagonal-block inverse of every panel, and where each supernode's panel
+// inverses start (sum over earlier panels of w^2)
+void build_inverse_schedule(const dct::Symbolic& S, int small_max,
+                            dct::Schedule* inv, std::vector<int64_t>* off,
+                            int64_t* total) {
+  off->assign(S.nsuper, 0);
+  int64_t acc = 0;
+  for (int s = 0; s < S.nsuper; ++s) {
+    (*off)[s] = acc;
+    const int ns = S.ns(s);
+    for (int p = 0; p * dct::kPanel < ns; ++p) {
+      const int64_t w = std::min(dct::kPanel, ns - p * dct::kPanel);
+      // large fronts store their inverses while factoring
+      if (S.front_n[s] <= small_max) inv->tasks.push_back({s, p, 0, 0});
+      acc += w * w;
+    }
+  }
+  *total = acc;
+  inv->launches.push_back({dct::kPanelInverse, 0, 0, int64_t(inv->tasks.size()), 0});
 }
 
 int upload_schedule(dct_plan* P, dct::Schedule* sch) {
@@ -352,7 +438,7 @@ cudaError_t dct::Profiler::collect() {
 }
 
 void dct::Profiler::reset() {
-  for (int k = 0; k < 8; ++k) {
+  for (int k = 0; k < kNumKinds; ++k) {
     ms[k] = fl[k] = by[k] = 0.0;
     n[k] = 0;
   }
@@ -448,14 +534,17 @@ int dct_symbolic_get_array(const dct_symbolic* h, const char* name, void* dst,
 int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t which,
                               int32_t* tasks, int64_t* ntasks, int64_t* launches,
                               int64_t* nlaunches) {
-  if (!h || !ntasks || !nlaunches || which < 0 || which > 2 ||
+  if (!h || !ntasks || !nlaunches || which < 0 || which > 3 ||
       (dtype != DCT_F64 && dtype != DCT_F32))
     return fail(DCT_ERR_ARG, "bad arguments");
-  dct::Schedule f, fw, bw;
+  dct::Schedule f, fw, bw, iv;
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(h->sym, small_max, &f);
-  build_solve_schedules(h->sym, &fw, &bw);
-  const dct::Schedule& sc = which == 0 ? f : (which == 1 ? fw : bw);
+  build_factor_schedule(h->sym, small_max, update_tile(dtype), &f);
+  build_solve_schedules(h->sym, dtype, &fw, &bw);
+  std::vector<int64_t> off;
+  int64_t tot = 0;
+  build_inverse_schedule(h->sym, small_max, &iv, &off, &tot);
+  const dct::Schedule& sc = which == 0 ? f : (which == 1 ? fw : (which == 2 ? bw : iv));
   const int64_t nt = int64_t(sc.tasks.size()), nl = int64_t(sc.launches.size());
   if (tasks) {
     if (*ntasks < nt) return fail(DCT_ERR_ARG, "task buffer too small");
@@ -527,19 +616,28 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
       (rc = upload(P, S.in_crow, &D.crow)) || (rc = upload(P, S.in_col, &D.col)))
     return bail(rc);
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(S, small_max, &P->fact);
-  build_solve_schedules(S, &P->fwd, &P->bwd);
-  account_factor(S, &P->fact, double(esize(dtype)));
+  build_factor_schedule(S, small_max, update_tile(dtype), &P->fact);
+  build_solve_schedules(S, dtype, &P->fwd, &P->bwd);
+  std::vector<int64_t> dinv_off;
+  build_inverse_schedule(S, small_max, &P->inv, &dinv_off, &P->dinv_stride);
+  {
+    const int64_t* d = nullptr;
+    if ((rc = upload(P, dinv_off, &d))) return bail(rc);
+    P->d_dinv_off = d;
+  }
+  account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype));
   account_solve(S, &P->fwd, double(esize(dtype)));
   account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||
-      (rc = upload_schedule(P, &P->bwd)))
+      (rc = upload_schedule(P, &P->bwd)) || (rc = upload_schedule(P, &P->inv)))
     return bail(rc);
   const size_t es = esize(dtype);
   P->front_stride = S.front_total;
   const size_t work = size_t(nbatch) * S.n * max_rhs;
   void* p = nullptr;
   if ((rc = alloc(P, es * S.front_total * nbatch, &P->fronts, "front storage")))
+    return bail(rc);
+  if ((rc = alloc(P, es * P->dinv_stride * nbatch, &P->dinv, "panel inverses")))
     return bail(rc);
   if ((rc = alloc(P, es * work, &P->bufA, "work buffer A"))) return bail(rc);
   if ((rc = alloc(P, es * work, &P->bufB, "work buffer B"))) return bail(rc);
@@ -689,7 +787,7 @@ int dct_plan_profile(dct_plan* P, int32_t enable, int32_t reset) {
 
 int dct_plan_profile_get(dct_plan* P, int32_t kind, double* ms, int64_t* launches,
                          double* flops, double* bytes) {
-  if (!P || kind < 0 || kind > 7) return fail(DCT_ERR_ARG, "bad arguments");
+  if (!P || kind < 0 || kind >= dct::kNumKinds) return fail(DCT_ERR_ARG, "bad arguments");
   int rc = set_device(P->device);
   if (rc) return rc;
   DCT_CUDA(P->prof.collect(), "profile collect");

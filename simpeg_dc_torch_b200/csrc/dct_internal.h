@@ -48,13 +48,20 @@ enum LaunchKind : int {
   kFwdStep,          // forward substitution, one panel step
   kBwdGemm,          // backward: subtract boundary-row contributions
   kBwdStep,          // backward substitution, one panel step
+  kFwdSmall,         // forward substitution of single-panel supernodes
+  kBwdSmall,         // backward substitution of single-panel supernodes
+  kPanelInverse,     // inverses of the factored diagonal blocks
+  kFwdTc,            // forward row-tile updates on tensor cores (float32)
+  kNumKinds
 };
 
 // Limits of the single-CTA front kernel (front fully in shared memory).
 constexpr int kSmallFrontF64 = 160;
 constexpr int kSmallFrontF32 = 224;
 constexpr int kThreads = 256;
-constexpr int kRhsChunk = 32;   // right-hand sides per CTA in the solves
+constexpr int kRhsChunk = 64;   // right-hand sides per CTA in the solves
+constexpr int kRowGroup = 4;    // 64-row tiles per CTA in forward panel steps
+constexpr int kUpdateTile = 64;   // trailing-update tile (rows = cols)
 
 struct Schedule {
   std::vector<PanelTask> tasks;    // host copy
@@ -78,8 +85,8 @@ struct Profiler {
   };
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
-  double ms[8] = {0}, fl[8] = {0}, by[8] = {0};
-  int64_t n[8] = {0};
+  double ms[kNumKinds] = {0}, fl[kNumKinds] = {0}, by[kNumKinds] = {0};
+  int64_t n[kNumKinds] = {0};
   cudaError_t begin(int kind, double flops, double bytes, cudaStream_t st);
   cudaError_t end(cudaStream_t st);
   cudaError_t collect();
@@ -102,6 +109,10 @@ struct dct_plan {
   dct::Schedule fact;              // factorization schedule
   dct::Schedule fwd;               // forward substitution schedule
   dct::Schedule bwd;               // backward substitution schedule
+  dct::Schedule inv;               // diagonal-block inverses (one launch)
+  void* dinv = nullptr;            // nbatch * dinv_stride elements of dtype
+  int64_t dinv_stride = 0;         // per system: sum over panels of w^2
+  const int64_t* d_dinv_off = nullptr;   // per supernode, first panel inverse
   void* bufA = nullptr;            // dtype, nbatch*n*max_rhs (work buffer A)
   void* bufB = nullptr;            // dtype, nbatch*n*max_rhs (work buffer B)
   double* x64 = nullptr;           // f32 plans: refined solution (dct_solve)

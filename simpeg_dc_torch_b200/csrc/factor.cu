@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 
 #include "dct_internal.h"
+#include "tile_mm.cuh"
+#include "tc_common.cuh"
 
 namespace dct {
 namespace {
@@ -142,19 +144,32 @@ k_large_extend_add(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   const int32_t* rel = S.rel + S.rel_ptr[c];
   const int64_t dst_col = int64_t(rel[j]) * N;
   const T* src = U + (nsc + j) * int64_t(nc) + nsc;
-  for (int i = j + lane; i < nbc; i += 32) F[rel[i] + dst_col] += src[i];
+  // batches of 4 per lane: loads before stores (F and U share one buffer)
+  for (int i0 = j + lane; i0 < nbc; i0 += 4 * 32) {
+    T sv[4], fv[4];
+    int64_t at[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + 32 * u;
+      at[u] = i < nbc ? rel[i] + dst_col : -1;
+      sv[u] = i < nbc ? src[i] : T(0);
+      fv[u] = i < nbc ? F[at[u]] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (at[u] >= 0) F[at[u]] = fv[u] + sv[u];
+  }
 }
 
 // ------------------------------------------------------------ large: panels
 // Factor the w x w diagonal block D (column-major, ld 64) in shared memory.
 template <typename T>
-__device__ void potrf_smem(T* D, int w, T* dsh, int* status, int s, int b,
-                           bool report) {
+__device__ void potrf_smem(T* D, int w, T* dsh, int* status, int s, int b) {
   const int tid = threadIdx.x;
   for (int k = 0; k < w; ++k) {
     T piv = D[k + k * kPanel];
     if (!good_pivot(piv)) {
-      if (report && tid == 0) flag_pivot(status, s, b);
+      if (tid == 0) flag_pivot(status, s, b);
       piv = T(1);
     }
     const T d = sqrt(piv);
@@ -175,18 +190,61 @@ __device__ void potrf_smem(T* D, int w, T* dsh, int* status, int s, int b,
   __syncthreads();
 }
 
-// task: s, p = panel, t0 >= 1 -> TRSM of row tile t0-1 of the rows below the
-// panel.  Every CTA factors the (still unfactored) diagonal block itself; the
-// factored block is written by the next launch (k_large_update, t0 = -1), so
-// no CTA of this launch can observe it half written.
+// X = D^{-1} for the factored lower block D (both ld 64): one thread per
+// column j runs the forward substitution D x = e_j.
+template <typename T>
+__device__ void trinv_smem(const T* D, int w, T* X) {
+  const int j = threadIdx.x;
+  if (j < w) {
+    for (int i = 0; i < j; ++i) X[i + j * kPanel] = T(0);
+    X[j + j * kPanel] = T(1) / D[j + j * kPanel];
+    for (int i = j + 1; i < w; ++i) {
+      T acc = T(0);
+      for (int q = j; q < i; ++q) acc += D[i + q * kPanel] * X[q + j * kPanel];
+      X[i + j * kPanel] = -acc / D[i + i * kPanel];
+    }
+  }
+  __syncthreads();
+}
+
+// Factor the diagonal block of the panel starting at column c0 (width w) of
+// front F (order N): L_pp is written back into F (lower part) and D_p^{-1}
+// (w x w, ld w) to `inv`.  Needs kDiagSmemElems elements of shared memory.
+constexpr int kDiagSmemElems = 2 * kPanel * kPanel + kPanel;
+template <typename T>
+__device__ void factor_diag(T* F, int N, int c0, int w, T* sm, T* inv,
+                            int* status, int s, int b) {
+  T* D = sm;
+  T* X = sm + kPanel * kPanel;
+  T* dsh = X + kPanel * kPanel;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
+    const int r = idx % kPanel, c = idx / kPanel;
+    D[idx] = (r < w && c < w && r >= c) ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
+  }
+  __syncthreads();
+  potrf_smem(D, w, dsh, status, s, b);
+  for (int idx = tid; idx < w * w; idx += blockDim.x) {
+    const int r = idx % w, c = idx / w;
+    if (r >= c) F[(c0 + r) + int64_t(c0 + c) * N] = D[r + c * kPanel];
+  }
+  trinv_smem(D, w, X);
+  for (int idx = tid; idx < w * w; idx += blockDim.x) {
+    const int r = idx % w, c = idx / w;
+    inv[r + c * w] = X[r + c * kPanel];
+  }
+}
+
+// task: s, p, t0 >= 1: the 64-row tile t0-1 below panel p becomes
+// F_rows D_p^{-T}, using the inverse stored when the diagonal was factored.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
-              int64_t front_stride, int* status) {
+              int64_t front_stride, const T* dinv, const int64_t* dinv_off,
+              int64_t dinv_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* X = D + kPanel * kPanel;
-  T* dsh = X + kPanel * kPanel;
+  T* S1 = reinterpret_cast<T*>(smem_raw);   // [q][c] = Dinv[c, q]
+  T* S2 = S1 + kPanel * kPanel;              // [q][r] = F[r, q]
   const PanelTask tk = tasks[blockIdx.x];
   const int b = blockIdx.y;
   const int s = tk.s;
@@ -195,47 +253,48 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   const int c0 = tk.p * kPanel;
   const int w = min(kPanel, ns - c0);
   T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-    const int r = idx % kPanel, c = idx / kPanel;
-    D[idx] = (r < w && c < w && r >= c) ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
-  }
-  __syncthreads();
-  potrf_smem(D, w, dsh, status, s, b, false);
+  const T* Di = dinv + int64_t(b) * dinv_stride + dinv_off[s] +
+                int64_t(tk.p) * kPanel * kPanel;
   const int r0 = c0 + w + (tk.t0 - 1) * kPanel;
   const int nr = min(kPanel, N - r0);
-  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-    const int r = idx % kPanel, c = idx / kPanel;
-    X[idx] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c0 + c) * N] : T(0);
+  for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+    const int a = idx % kPanel, q = idx / kPanel;
+    S1[idx] = (a < w && q < w) ? Di[a + q * w] : T(0);
+    S2[idx] = (a < nr && q < w) ? F[(r0 + a) + int64_t(c0 + q) * N] : T(0);
   }
   __syncthreads();
-  // X <- X D^{-T}: row r solves D x = a, one thread per row
-  if (tid < nr) {
-    const int r = tid;
-    for (int c = 0; c < w; ++c) {
-      T acc = X[r + c * kPanel];
-      for (int q = 0; q < c; ++q) acc -= D[c + q * kPanel] * X[r + q * kPanel];
-      X[r + c * kPanel] = acc / D[c + c * kPanel];
+  T acc[4][4];
+  zero_acc(acc);
+  mm64<T, kPanel, kPanel>(S1, S2, w, w, acc);
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int c = ag + 16 * p;
+    if (c >= w) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = jg + 16 * q;
+      if (r < nr) F[(r0 + r) + int64_t(c0 + c) * N] = acc[p][q];
     }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < nr * w; idx += blockDim.x) {
-    const int r = idx % nr, c = idx / nr;
-    F[(r0 + r) + int64_t(c0 + c) * N] = X[r + c * kPanel];
   }
 }
 
-// task: s, p = panel, t0 = tile row i, t1 = tile col j (i >= j) of the
-// trailing block that starts after the panel: F_ij -= L_i L_j^T.
-// t0 = -1: factor the panel's diagonal block and write it (no other task of
-// this launch reads or writes that block).
+// task: s, p, t0 = i, t1 = j (i >= j): 64 x 64 tile of the trailing block
+// that starts after panel p, F_ij -= L_i L_j^T with K = w (4 x 4 outputs per
+// thread, rows on the fast thread index so the tile is written coalesced).
+// The CTA of tile (0, 0) -- the next panel's diagonal block -- factors that
+// block after its own update (no other task of the launch touches it).
+// t0 = -1: factor the diagonal block of panel p itself (a front's first panel).
+constexpr int kUT = kUpdateTile;
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
-               int64_t front_stride, int* status) {
+               int64_t front_stride, T* dinv, const int64_t* dinv_off,
+               int64_t dinv_stride, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);   // [k][row], ld kPanel
-  T* Bs = As + kPanel * kPanel;
+  T* As = reinterpret_cast<T*>(smem_raw);   // [k][row of tile i], ld 64
+  T* Bs = As + kPanel * kUT;                // [k][row of tile j], ld 64
   const PanelTask tk = tasks[blockIdx.x];
   const int b = blockIdx.y;
   const int s = tk.s;
@@ -245,58 +304,197 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   const int w = min(kPanel, ns - c0);
   const int base = c0 + w;
   T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  T* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
   const int tid = threadIdx.x;
   if (tk.t0 < 0) {
-    T* D = As;
-    T* dsh = Bs;
-    for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-      const int r = idx % kPanel, c = idx / kPanel;
-      D[idx] = (r < w && c < w && r >= c) ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
-    }
-    __syncthreads();
-    potrf_smem(D, w, dsh, status, s, b, true);
-    for (int idx = tid; idx < w * w; idx += blockDim.x) {
-      const int r = idx % w, c = idx / w;
-      if (r >= c) F[(c0 + r) + int64_t(c0 + c) * N] = D[r + c * kPanel];
-    }
+    factor_diag(F, N, c0, w, As, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
     return;
   }
-  const int ri = base + tk.t0 * kPanel, rj = base + tk.t1 * kPanel;
-  const int ni = min(kPanel, N - ri), nj = min(kPanel, N - rj);
-  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-    const int r = idx % kPanel, k = idx / kPanel;
+  const int ri = base + tk.t0 * kUT, rj = base + tk.t1 * kUT;
+  const int ni = min(kUT, N - ri), nj = min(kUT, N - rj);
+  for (int idx = tid; idx < kPanel * kUT; idx += blockDim.x) {
+    const int r = idx % kUT, k = idx / kUT;
     const bool kin = k < w;
     As[idx] = (kin && r < ni) ? F[(ri + r) + int64_t(c0 + k) * N] : T(0);
     Bs[idx] = (kin && r < nj) ? F[(rj + r) + int64_t(c0 + k) * N] : T(0);
   }
   __syncthreads();
-  const int tx = tid & 15;   // rows tx + 16 a
-  const int ty = tid >> 4;   // cols ty + 16 c
   T acc[4][4];
+  zero_acc(acc);
+  mm64<T, kUT, kUT>(Bs, As, w, nj, acc);    // acc[p][q]: col ag+16p, row jg+16q
+  const int jg = tid & 15, ag = tid >> 4;
+  // all loads first, then the stores: the loads cannot be hoisted over
+  // stores to the same buffer, so a fused read-modify-write loop would
+  // serialise one global round trip per element
+  T cur[4][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int p = 0; p < 4; ++p)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) acc[a][c] = T(0);
-  for (int k = 0; k < w; ++k) {
-    T av[4], bv[4];
+    for (int q = 0; q < 4; ++q) {
+      const int cc = ag + 16 * p, rr = jg + 16 * q;
+      cur[p][q] = (cc < nj && rr < ni) ? F[(ri + rr) + int64_t(rj + cc) * N] : T(0);
+    }
 #pragma unroll
-    for (int a = 0; a < 4; ++a) av[a] = As[k * kPanel + tx + 16 * a];
+  for (int p = 0; p < 4; ++p)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) bv[c] = Bs[k * kPanel + ty + 16 * c];
+    for (int q = 0; q < 4; ++q) {
+      const int cc = ag + 16 * p, rr = jg + 16 * q;
+      if (cc < nj && rr < ni) F[(ri + rr) + int64_t(rj + cc) * N] = cur[p][q] - acc[p][q];
+    }
+  if (tk.t0 == 0 && tk.t1 == 0 && base < ns) {
+    __syncthreads();   // this CTA's updates of the block are complete
+    factor_diag(F, N, base, min(kPanel, ns - base), As,
+                Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
+  }
+}
+
+// ------------------------------------------------------------ tensor cores
+// float32 fronts: the 128 x 128 trailing-update tile F_ij -= L_i L_j^T on the
+// 5th-generation tensor cores (tcgen05.mma kind::tf32, accumulator in TMEM).
+// Each float32 operand x is split as x_hi = tf32(x), x_lo = tf32(x - x_hi),
+// and the product is x_hi y_hi + x_hi y_lo + x_lo y_hi (the 3xTF32 scheme of
+// Markidis et al., 2018, and Ootomo & Yokota, 2022), which restores float32
+// accuracy from TF32 products accumulated in float32.
+//
+// Shared-memory operands are K-major without swizzle: core matrices of
+// 8 rows x 16 bytes (4 values), element (m, k) at byte
+//   (m / 8) * SBO + (k / 4) * LBO + (m % 8) * 16 + (k % 4) * 4,
+// LBO = 128 (next 4 values of k), SBO = 2048 (next 8 rows; 64 values of k).
+// One MMA covers K = 8: its descriptors start 256 bytes further per step.
+// split the rows [r0, r0+nr) x columns [c0, c0+w) of front F (float) into the
+// hi/lo K-major operands at `hi`/`lo` (zero beyond nr rows and w columns).
+// Lane l of a warp handles row m_lo = l / 4 and column k_lo = l % 4 of one
+// 8 x 4 core matrix, so each warp stores one contiguous 128-byte block per
+// operand (no bank conflicts) and reads four 32-byte pieces of the front.
+__device__ __forceinline__ void load_split(const float* __restrict__ F, int N, int r0,
+                                           int nr, int c0, int w, unsigned char* hi,
+                                           unsigned char* lo) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kWarps = kTcThreads / 32;
+  constexpr int kCores = (kTcM / 8) * (kPanel / 4);   // 16 x 16 core matrices
+  constexpr int kPer = kCores / kWarps;
+  const int m_lo = lane >> 2, k_lo = lane & 3;   // lane = m_lo * 4 + k_lo
+  // every load of this warp is issued before any shared store
+  float v[kPer];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[a][c] += av[a] * bv[c];
+  for (int u = 0; u < kPer; ++u) {
+    const int cm = warp + u * kWarps;
+    const int m = (cm % (kTcM / 8)) * 8 + m_lo, k = (cm / (kTcM / 8)) * 4 + k_lo;
+    v[u] = (m < nr && k < w) ? F[(r0 + m) + int64_t(c0 + k) * N] : 0.0f;
   }
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int cc = ty + 16 * c;
-    if (cc >= nj) continue;
+  for (int u = 0; u < kPer; ++u) {
+    const int cm = warp + u * kWarps;
+    tc_store_split(hi, lo, (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
+                   v[u]);
+  }
+}
+
+// task: s, p, t0 = i, t1 = j (i >= j) over 128-row tiles of the trailing
+// block after panel p, or t0 = -1: factor the diagonal block of panel p.
+// The CTA of tile (0, 0) factors the next panel's diagonal block afterwards.
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
+                  int64_t front_stride, float* dinv, const int64_t* dinv_off,
+                  int64_t dinv_stride, int* status) {
+  // dynamic shared memory is 16-byte aligned, all the descriptors need;
+  // addressing it directly keeps the accesses in the shared state space
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* base_ptr = smem_raw;
+  unsigned char* Ahi = base_ptr;
+  unsigned char* Alo = Ahi + kTcOperandBytes;
+  unsigned char* Bhi = Alo + kTcOperandBytes;
+  unsigned char* Blo = Bhi + kTcOperandBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcOperandBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+
+  const PanelTask tk = tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s;
+  const int N = S.front_n[s];
+  const int ns = S.sn_first[s + 1] - S.sn_first[s];
+  const int c0 = tk.p * kPanel;
+  const int w = min(kPanel, ns - c0);
+  const int base = c0 + w;
+  float* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  float* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float* sm = reinterpret_cast<float*>(base_ptr);
+  if (tk.t0 < 0) {
+    factor_diag(F, N, c0, w, sm, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
+    return;
+  }
+  const int ri = base + tk.t0 * kTcM, rj = base + tk.t1 * kTcN;
+  const int ni = min(kTcM, N - ri), nj = min(kTcN, N - rj);
+
+  if (warp == 0) tmem_alloc(tmem_slot, kTcN);
+  if (tid == 0) mbar_init(mbar);
+  load_split(F, N, ri, ni, c0, w, Ahi, Alo);
+  load_split(F, N, rj, nj, c0, w, Bhi, Blo);
+  tc_publish_smem();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0)
+    umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
+                (w + 7) / 8, umma_idesc_tf32(kTcM, kTcN), 0, mbar);
+  const bool done = tc_wait(mbar, 0, status, DCT_ERR_DEVICE_TIMEOUT, s, b);
+  if (done) {
+    // warp w reads TMEM lanes (tile rows) 32(w%4) .. +31, columns 32(w/4) .. +31
+    const int row = (warp & 3) * 32 + lane;
+    const int cb = (warp >> 2) * 32;
+    uint32_t v[32];
+    tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+    if (row < ni) {
+      float* dst = F + (ri + row) + int64_t(rj + cb) * N;
+      float cur[32];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int rr = tx + 16 * a;
-      if (rr < ni) F[(ri + rr) + int64_t(rj + cc) * N] -= acc[a][c];
+      for (int c = 0; c < 32; ++c) cur[c] = (cb + c < nj) ? dst[int64_t(c) * N] : 0.0f;
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        if (cb + c < nj) dst[int64_t(c) * N] = cur[c] - __uint_as_float(v[c]);
     }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTcN);
+  if (done && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
+    __syncthreads();   // this CTA's updates of the block are complete
+    factor_diag(F, N, base, min(kPanel, ns - base), sm,
+                Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
+  }
+}
+
+constexpr size_t kTcSmem = 4 * size_t(kTcOperandBytes) + 64;
+static_assert(4 * size_t(kTcOperandBytes) >= sizeof(float) * kDiagSmemElems,
+              "tensor-core update smem must also hold factor_diag's workspace");
+
+// task: s, p.  D_p^{-1} of the factored diagonal block of panel p of a small
+// front, written column-major (ld w) at dinv + dinv_off[s] + p*64*64.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_panel_inverse(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
+                int64_t front_stride, T* dinv, const int64_t* dinv_off,
+                int64_t dinv_stride) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* L = reinterpret_cast<T*>(smem_raw);       // ld kPanel
+  T* X = L + kPanel * kPanel;                   // ld kPanel
+  const PanelTask tk = tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s;
+  const int N = S.front_n[s];
+  const int ns = S.sn_first[s + 1] - S.sn_first[s];
+  const int c0 = tk.p * kPanel;
+  const int w = min(kPanel, ns - c0);
+  const T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+    const int r = idx % w, c = idx / w;
+    L[r + c * kPanel] = r >= c ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
+  }
+  __syncthreads();
+  trinv_smem(L, w, X);
+  T* out = dinv + int64_t(b) * dinv_stride + dinv_off[s] + int64_t(tk.p) * kPanel * kPanel;
+  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+    const int r = idx % w, c = idx / w;
+    out[r + c * w] = X[r + c * kPanel];
   }
 }
 
@@ -310,8 +508,10 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
   if (e != cudaSuccess) return e;
   const int small_max = sizeof(T) == 8 ? kSmallFrontF64 : kSmallFrontF32;
   const size_t small_smem = sizeof(T) * (size_t(small_max) * small_max + small_max);
-  const size_t panel_smem = sizeof(T) * (2 * kPanel * kPanel + kPanel);
-  const size_t update_smem = sizeof(T) * (2 * kPanel * kPanel);
+  const size_t panel_smem = sizeof(T) * (2 * kPanel * kPanel);
+  // the update kernel's tiles, or factor_diag's D, X and pivots, whichever is larger
+  static_assert(2 * kPanel * kUT + kPanel >= kDiagSmemElems, "update smem too small");
+  const size_t update_smem = sizeof(T) * (2 * kPanel * kUT + kPanel);
   // attributes are per device: set them on every call (cheap host calls)
   e = cudaFuncSetAttribute(k_small_front<T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -324,6 +524,10 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
     e = cudaFuncSetAttribute(k_large_update<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(update_smem));
+  if (e == cudaSuccess && sizeof(T) == 4)
+    e = cudaFuncSetAttribute(k_large_update_tc,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kTcSmem));
   if (e != cudaSuccess) return e;
   const PanelTask* tasks = P->fact.d_tasks;
   for (size_t li = 0; li < P->fact.launches.size(); ++li) {
@@ -351,16 +555,45 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                                                          P->front_stride);
         break;
       case kLargePanel:
-        k_large_panel<T><<<grid, kThreads, panel_smem, st>>>(P->ds, t, fronts,
-                                                    P->front_stride, P->status);
+        k_large_panel<T><<<grid, kThreads, panel_smem, st>>>(
+            P->ds, t, fronts, P->front_stride, static_cast<const T*>(P->dinv),
+            P->d_dinv_off, P->dinv_stride);
         break;
       case kLargeUpdate:
-        k_large_update<T><<<grid, kThreads, update_smem, st>>>(
-            P->ds, t, fronts, P->front_stride, P->status);
+        if constexpr (sizeof(T) == 4) {
+          k_large_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(
+              P->ds, t, reinterpret_cast<float*>(fronts), P->front_stride,
+              static_cast<float*>(P->dinv), P->d_dinv_off, P->dinv_stride,
+              P->status);
+        } else {
+          k_large_update<T><<<grid, kThreads, update_smem, st>>>(
+              P->ds, t, fronts, P->front_stride, static_cast<T*>(P->dinv),
+              P->d_dinv_off, P->dinv_stride, P->status);
+        }
         break;
       default:
         return cudaErrorInvalidValue;
     }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = P->prof.end(st);
+    if (e != cudaSuccess) return e;
+  }
+  // inverses of the diagonal blocks of small fronts, for the substitution
+  // (large fronts store theirs while factoring)
+  const size_t inv_smem = sizeof(T) * 2 * kPanel * kPanel;
+  e = cudaFuncSetAttribute(k_panel_inverse<T>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(inv_smem));
+  if (e != cudaSuccess) return e;
+  const int64_t ninv = int64_t(P->inv.tasks.size());
+  if (ninv > 0) {
+    e = P->prof.begin(kPanelInverse, 0.0, 0.0, st);
+    if (e != cudaSuccess) return e;
+    k_panel_inverse<T><<<dim3(static_cast<unsigned>(ninv), nb), kThreads, inv_smem,
+                         st>>>(P->ds, P->inv.d_tasks, fronts, P->front_stride,
+                               static_cast<T*>(P->dinv), P->d_dinv_off,
+                               P->dinv_stride);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = P->prof.end(st);

@@ -1,225 +1,527 @@
 // Multi-RHS supernodal substitution L L^T x = b for nbatch systems, in the
 // permuted order, on row-major (n, k) right-hand sides.
 //
+// The inverse of every 64-column panel's diagonal block, D_p^{-1}, is formed
+// once after the factorization (k_panel_inverse), so each panel solve is a
+// small matrix product instead of a serial triangular sweep.
+//
 // Two work buffers A and B of nbatch*n*k elements are used so that no launch
 // ever reads a location that another CTA of the same launch writes:
-//   forward  (levels bottom-up, panel steps in order): the right-hand side b
-//            lives in A and receives the updates -L_below y_p (plain stores for
-//            rows of the same supernode, atomics for its boundary rows, which
-//            other supernodes of the level may also update); the solved panel
-//            y_p = D_p^{-1} b_p is written to B.
-//   backward (levels top-down): first y_p -= L_{B,p}^T x_B for every panel
-//            (x_B are final rows of ancestors, in A); then panel steps from the
-//            last panel down: x_p = D_p^{-T} y_p is written to A and
+//   forward  (levels bottom-up): the right-hand side b lives in A and receives
+//            the updates -L_below y_p (plain stores for rows of the same
+//            supernode, atomics for its boundary rows, which other supernodes
+//            of the level may also update); y_p = D_p^{-1} b_p goes to B.
+//   backward (levels top-down): y_p -= L_{B,p}^T x_B (x_B: final rows of
+//            ancestors, in A); x_p = D_p^{-T} y_p goes to A and
 //            y_i -= L_{p,i}^T x_p updates the earlier panels in B.
-// Each CTA of a step recomputes the small triangular solve of its panel
-// instead of waiting for another CTA: no inter-CTA synchronisation exists.
+// Supernodes of one panel are handled by one CTA per (supernode, system,
+// 64 right-hand sides) in each direction.  Larger supernodes run panel steps
+// whose CTAs recompute the panel's small product instead of waiting for
+// another CTA: no inter-CTA synchronisation exists anywhere.
 #include <cuda_runtime.h>
 
 #include "dct_internal.h"
+#include "tile_mm.cuh"
+#include "tc_common.cuh"
 
 namespace dct {
 namespace {
+
+constexpr int kRC = kRhsChunk;          // right-hand sides per CTA (64)
+constexpr int kLD = kPanel;             // leading dimension of smem tiles
 
 template <typename T>
 __device__ __forceinline__ void atomic_sub(T* p, T v) {
   atomicAdd(p, -v);
 }
 
-// Load the lower triangle of the w x w diagonal block of panel p (column-major,
-// ld 64) and the panel's right-hand-side rows (w x rc, ld kRhsChunk+1).
+// S1 (the "a" operand) uses a padded leading dimension: several loaders
+// store it transposed, which would otherwise hit one bank 32 times.
+constexpr int kLD1 = kLD + 1;
+
 template <typename T>
-__device__ void load_panel(const T* F, int N, int c0, int w, T* D,
-                           const T* src, int64_t rowbase, int k, int j0, int rc,
-                           T* Y) {
-  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-    const int r = idx % w, c = idx / w;
-    D[r + c * kPanel] = r >= c ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
-  }
-  for (int idx = threadIdx.x; idx < w * rc; idx += blockDim.x) {
-    const int r = idx / rc, j = idx % rc;
-    Y[r * (kRhsChunk + 1) + j] = src[(rowbase + r) * k + j0 + j];
+__device__ __forceinline__ void mm_tile(const T* __restrict__ S1,
+                                        const T* __restrict__ S2, int K,
+                                        int arows, T (&acc)[4][4]) {
+  mm64<T, kLD1, kLD>(S1, S2, K, arows, acc);
+}
+
+// rows [r0, r0+nr) x right-hand sides [j0, j0+rc) of a (n, k) buffer into
+// S[r][j] (ld kLD), zero elsewhere; rows may be gathered through `map`.
+template <typename T>
+__device__ __forceinline__ void load_rhs(T* S, const T* __restrict__ src, int k,
+                                         int j0, int rc, int nr,
+                                         const int32_t* map, int64_t r0) {
+  for (int idx = threadIdx.x; idx < kLD * kRC; idx += blockDim.x) {
+    const int r = idx / kRC, j = idx % kRC;
+    T v = T(0);
+    if (r < nr && j < rc) {
+      const int64_t row = map ? int64_t(map[r]) : r0 + r;
+      v = src[row * k + j0 + j];
+    }
+    S[r * kLD + j] = v;
   }
 }
 
-// ------------------------------------------------------------ forward step
-// task: s, p; t0 = 0 -> write y_p to B; t0 >= 1 -> row tile t0-1 below the
-// panel receives -L_tile y_p in A.
+// D^{-1} of panel p (w x w, column-major, ld w) as S[c][r] = Dinv[r, c]
+// (transposed = false: forward product) or S[r][c] = Dinv[r, c] (true).
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_fwd_step(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
-           int64_t front_stride, T* bufA, T* bufB, int n, int k, int nchunk) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* Y = D + kPanel * kPanel;
-  T* Lt = Y + kPanel * (kRhsChunk + 1);
-  const PanelTask tk = tasks[blockIdx.x];
-  const int b = blockIdx.y / nchunk;
-  const int j0 = (blockIdx.y % nchunk) * kRhsChunk;
-  const int rc = min(kRhsChunk, k - j0);
-  const int s = tk.s;
-  const int N = S.front_n[s];
-  const int first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int c0 = tk.p * kPanel;
-  const int w = min(kPanel, ns - c0);
-  const T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  T* A = bufA + int64_t(b) * n * k;
-  T* Bo = bufB + int64_t(b) * n * k;
-  load_panel(F, N, c0, w, D, A, int64_t(first + c0), k, j0, rc, Y);
-  __syncthreads();
-  // forward substitution, one thread per right-hand side
-  if (threadIdx.x < rc) {
-    const int j = threadIdx.x;
-    for (int c = 0; c < w; ++c) {
-      T acc = Y[c * (kRhsChunk + 1) + j];
-      for (int q = 0; q < c; ++q) acc -= D[c + q * kPanel] * Y[q * (kRhsChunk + 1) + j];
-      Y[c * (kRhsChunk + 1) + j] = acc / D[c + c * kPanel];
-    }
-  }
-  __syncthreads();
-  if (tk.t0 == 0) {
-    for (int idx = threadIdx.x; idx < w * rc; idx += blockDim.x) {
-      const int r = idx / rc, j = idx % rc;
-      Bo[int64_t(first + c0 + r) * k + j0 + j] = Y[r * (kRhsChunk + 1) + j];
-    }
-    return;
-  }
-  const int r0 = c0 + w + (tk.t0 - 1) * kPanel;
-  const int nr = min(kPanel, N - r0);
-  for (int idx = threadIdx.x; idx < nr * w; idx += blockDim.x) {
-    const int r = idx % nr, c = idx / nr;
-    Lt[r + c * kPanel] = F[(r0 + r) + int64_t(c0 + c) * N];
-  }
-  __syncthreads();
-  const int32_t* rows = S.rows + S.rows_ptr[s];
-  for (int idx = threadIdx.x; idx < nr * rc; idx += blockDim.x) {
-    const int r = idx / rc, j = idx % rc;
-    T acc = T(0);
-    for (int c = 0; c < w; ++c) acc += Lt[r + c * kPanel] * Y[c * (kRhsChunk + 1) + j];
-    const int lr = r0 + r;
-    T* dst = A + int64_t(rows[lr]) * k + j0 + j;
-    if (lr < ns) *dst -= acc;
-    else atomic_sub(dst, acc);
+__device__ __forceinline__ void load_dinv(T* S, const T* __restrict__ Di, int w,
+                                          bool transposed) {
+  for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+    const int r = idx % kLD, c = idx / kLD;
+    const T v = (r < w && c < w) ? Di[r + c * w] : T(0);
+    if (transposed) S[r * kLD1 + c] = v;
+    else S[c * kLD1 + r] = v;
   }
 }
 
-// ------------------------------------------------------------ backward gemm
-// task: s, p: y_p (in B) -= L[boundary rows, panel p]^T x[boundary rows] (A)
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_bwd_gemm(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
-           int64_t front_stride, const T* bufA, T* bufB, int n, int k,
-           int nchunk) {
+struct SolveArgs {
+  DevSym S;
+  const PanelTask* tasks;
+  const T* fronts;
+  int64_t front_stride;
+  const T* dinv;
+  const int64_t* dinv_off;
+  int64_t dinv_stride;
+  T* A;
+  T* B;
+  int n, k, nchunk;
+  int* status;
+};
+
+// ------------------------------------------------------------ forward, small
+// one CTA: y = D^{-1} b (to B), then b[boundary rows] -= L_B y (atomics, A)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fwd_small(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Lt = reinterpret_cast<T*>(smem_raw);          // [row][col], ld kPanel
-  T* Xt = Lt + kPanel * kPanel;                     // [row][j], ld kRhsChunk+1
-  const PanelTask tk = tasks[blockIdx.x];
-  const int b = blockIdx.y / nchunk;
-  const int j0 = (blockIdx.y % nchunk) * kRhsChunk;
-  const int rc = min(kRhsChunk, k - j0);
-  const int s = tk.s;
-  const int N = S.front_n[s];
-  const int first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int nbd = N - ns;
-  const int c0 = tk.p * kPanel;
-  const int w = min(kPanel, ns - c0);
-  const T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  const T* A = bufA + int64_t(b) * n * k;
-  T* Bo = bufB + int64_t(b) * n * k;
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  T* Y = S2 + kLD * kLD;
+  const int s = g.tasks[blockIdx.x].s;
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int w = S.sn_first[s + 1] - first;
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s], w, false);
+  load_rhs(S2, A, g.k, j0, rc, w, nullptr, first);
+  __syncthreads();
+  T acc[4][4];
+  zero_acc(acc);
+  mm_tile(S1, S2, w, w, acc);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ag + 16 * p, j = jg + 16 * q;
+      Y[r * kLD + j] = acc[p][q];
+      if (r < w && j < rc) Bo[int64_t(first + r) * g.k + j0 + j] = acc[p][q];
+    }
   const int32_t* rows = S.rows + S.rows_ptr[s];
-  // each thread owns outputs (c, j) = idx, idx + 256, ...
-  constexpr int kOut = (kPanel * kRhsChunk + kThreads - 1) / kThreads;
-  T acc[kOut];
-#pragma unroll
-  for (int u = 0; u < kOut; ++u) acc[u] = T(0);
-  for (int i0 = 0; i0 < nbd; i0 += kPanel) {
-    const int ni = min(kPanel, nbd - i0);
+  for (int r0 = w; r0 < N; r0 += kLD) {
+    const int nr = min(kLD, N - r0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < ni * w; idx += blockDim.x) {
-      const int r = idx % ni, c = idx / ni;
-      Lt[r * kPanel + c] = F[(ns + i0 + r) + int64_t(c0 + c) * N];
-    }
-    for (int idx = threadIdx.x; idx < ni * rc; idx += blockDim.x) {
-      const int r = idx / rc, j = idx % rc;
-      Xt[r * (kRhsChunk + 1) + j] = A[int64_t(rows[ns + i0 + r]) * k + j0 + j];
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int r = idx % kLD, c = idx / kLD;
+      S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c) * N] : T(0);
     }
     __syncthreads();
+    zero_acc(acc);
+    mm_tile(S1, Y, w, nr, acc);
 #pragma unroll
-    for (int u = 0; u < kOut; ++u) {
-      const int idx = threadIdx.x + u * kThreads;
-      const int c = idx / kRhsChunk, j = idx % kRhsChunk;
-      if (c < w && j < rc) {
-        T a = acc[u];
-        for (int r = 0; r < ni; ++r)
-          a += Lt[r * kPanel + c] * Xt[r * (kRhsChunk + 1) + j];
-        acc[u] = a;
+    for (int p = 0; p < 4; ++p) {
+      const int r = ag + 16 * p;
+      if (r >= nr) continue;
+      T* dst = A + int64_t(rows[r0 + r]) * g.k + j0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = jg + 16 * q;
+        if (j < rc) atomic_sub(dst + j, acc[p][q]);
       }
     }
   }
+}
+
+// ------------------------------------------------------------ forward, step
+// large supernodes, panel p.  t0 = 0: y_p = D_p^{-1} b_p to B.  t0 >= 1: row
+// tiles [t0-1, t1) below the panel (64 rows each) receive -L y_p in A.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fwd_step(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  T* Y = S2 + kLD * kLD;
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s] + int64_t(tk.p) * kPanel * kPanel,
+            w, false);
+  load_rhs(S2, A, g.k, j0, rc, w, nullptr, first + c0);
+  __syncthreads();
+  T acc[4][4];
+  zero_acc(acc);
+  mm_tile(S1, S2, w, w, acc);
+  if (tk.t0 == 0) {
 #pragma unroll
-  for (int u = 0; u < kOut; ++u) {
-    const int idx = threadIdx.x + u * kThreads;
-    const int c = idx / kRhsChunk, j = idx % kRhsChunk;
-    if (c < w && j < rc) Bo[int64_t(first + c0 + c) * k + j0 + j] -= acc[u];
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = ag + 16 * p, j = jg + 16 * q;
+        if (r < w && j < rc) Bo[int64_t(first + c0 + r) * g.k + j0 + j] = acc[p][q];
+      }
+    return;
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Y[(ag + 16 * p) * kLD + jg + 16 * q] = acc[p][q];
+  const int32_t* rows = S.rows + S.rows_ptr[s];
+  for (int t = tk.t0 - 1; t < tk.t1; ++t) {
+    const int r0 = c0 + w + t * kLD;
+    const int nr = min(kLD, N - r0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int r = idx % kLD, c = idx / kLD;
+      S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c0 + c) * N] : T(0);
+    }
+    __syncthreads();
+    zero_acc(acc);
+    mm_tile(S1, Y, w, nr, acc);
+    T cur[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int r = ag + 16 * p;
+      const bool own = r < nr && r0 + r < ns;
+      const T* src = own ? A + int64_t(rows[r0 + r]) * g.k + j0 : nullptr;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = jg + 16 * q;
+        cur[p][q] = (own && j < rc) ? src[j] : T(0);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const int r = ag + 16 * p;
+      if (r >= nr) continue;
+      const int lr = r0 + r;
+      T* dst = A + int64_t(rows[lr]) * g.k + j0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = jg + 16 * q;
+        if (j >= rc) continue;
+        if (lr < ns) dst[j] = cur[p][q] - acc[p][q];
+        else atomic_sub(dst + j, acc[p][q]);
+      }
+    }
   }
 }
 
-// ------------------------------------------------------------ backward step
-// task: s, p; t0 = i <= p.  i == p -> write x_p to A; i < p -> y_i (in B)
-// -= L[panel p rows, panel i cols]^T x_p.
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_bwd_step(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
-           int64_t front_stride, T* bufA, T* bufB, int n, int k, int nchunk) {
+// ------------------------------------------------------------ forward, tensor cores
+// float32 plans, large supernodes, panel p: one 128-row tile t0 below the
+// panel receives -L_tile y_p for up to 256 right-hand sides at once
+// (tcgen05.mma kind::tf32, 3xTF32, M = 128, N = right-hand sides rounded up
+// to 16).  y_p was written to B by the preceding launch (k_fwd_step, t0 = 0).
+constexpr int kTcRhs = 256;                              // N per CTA
+constexpr int kTcRhsBytes = kTcRhs * 64 * 4;             // one B operand
+constexpr size_t kFwdTcSmem = 2 * size_t(kTcOperandBytes) + 2 * size_t(kTcRhsBytes) + 64;
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_fwd_tc(SolveArgs<float> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  T* Y = D + kPanel * kPanel;
-  T* Lt = Y + kPanel * (kRhsChunk + 1);
-  const PanelTask tk = tasks[blockIdx.x];
-  const int b = blockIdx.y / nchunk;
-  const int j0 = (blockIdx.y % nchunk) * kRhsChunk;
-  const int rc = min(kRhsChunk, k - j0);
+  unsigned char* Ahi = smem_raw;
+  unsigned char* Alo = Ahi + kTcOperandBytes;
+  unsigned char* Bhi = Alo + kTcOperandBytes;
+  unsigned char* Blo = Bhi + kTcRhsBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcRhsBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kTcRhs;
+  const int kc = min(kTcRhs, g.k - j0);
+  const int np = (kc + 15) & ~15;
+  const DevSym& S = g.S;
   const int s = tk.s;
-  const int N = S.front_n[s];
-  const int first = S.sn_first[s];
+  const int N = S.front_n[s], first = S.sn_first[s];
   const int ns = S.sn_first[s + 1] - first;
-  const int c0 = tk.p * kPanel;
-  const int w = min(kPanel, ns - c0);
-  const T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  T* A = bufA + int64_t(b) * n * k;
-  T* Bo = bufB + int64_t(b) * n * k;
-  load_panel(F, N, c0, w, D, Bo, int64_t(first + c0), k, j0, rc, Y);
-  __syncthreads();
-  if (threadIdx.x < rc) {
-    const int j = threadIdx.x;
-    for (int c = w - 1; c >= 0; --c) {
-      T acc = Y[c * (kRhsChunk + 1) + j];
-      for (int q = c + 1; q < w; ++q) acc -= D[q + c * kPanel] * Y[q * (kRhsChunk + 1) + j];
-      Y[c * (kRhsChunk + 1) + j] = acc / D[c + c * kPanel];
+  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
+  const int r0 = c0 + w + tk.t0 * kTcM;
+  const int nr = min(kTcM, N - r0);
+  const float* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  float* A = g.A + int64_t(b) * g.n * g.k;
+  const float* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nwarps = blockDim.x >> 5;
+
+  if (warp == 0) tmem_alloc(tmem_slot, kTcRhs);
+  if (tid == 0) mbar_init(mbar);
+  // A: the L rows of the tile (m = tile row, k = panel column); all of a
+  // warp's loads are issued before its shared stores
+  {
+    constexpr int kWarps = kTcThreads / 32, kPer = (kTcM / 8) * 16 / kWarps;
+    const int m_lo = lane >> 2, k_lo = lane & 3;
+    float v[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int cm = warp + u * kWarps;
+      const int m = (cm % (kTcM / 8)) * 8 + m_lo, kq = (cm / (kTcM / 8)) * 4 + k_lo;
+      v[u] = (m < nr && kq < w) ? F[(r0 + m) + int64_t(c0 + kq) * N] : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int cm = warp + u * kWarps;
+      tc_store_split(Ahi, Alo,
+                     (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
+                     v[u]);
     }
   }
-  __syncthreads();
-  if (tk.t0 == tk.p) {
-    for (int idx = threadIdx.x; idx < w * rc; idx += blockDim.x) {
-      const int r = idx / rc, j = idx % rc;
-      A[int64_t(first + c0 + r) * k + j0 + j] = Y[r * (kRhsChunk + 1) + j];
+  // B: y_p^T (n = right-hand side, k = panel row), read row-wise from B
+  {
+    constexpr int kWarps = kTcThreads / 32;
+    const int ncm = (np / 8) * 16;
+    const int j_lo = lane >> 2, k_lo = lane & 3;
+    for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
+      float v[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int cm = c0m + warp + u * kWarps;
+        const int j = (cm % (np / 8)) * 8 + j_lo, kq = (cm / (np / 8)) * 4 + k_lo;
+        v[u] = (cm < ncm && j < kc && kq < w)
+                   ? Bo[int64_t(first + c0 + kq) * g.k + j0 + j] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 16; ++u) {
+        const int cm = c0m + warp + u * kWarps;
+        if (cm < ncm)
+          tc_store_split(Bhi, Blo,
+                         (cm % (np / 8)) * kTcSBO + (cm / (np / 8)) * kTcLBO + lane * 4,
+                         v[u]);
+      }
     }
+  }
+  tc_publish_smem();
+  const uint32_t tmem = *tmem_slot;
+  if (tid == 0)
+    umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
+                (w + 7) / 8, umma_idesc_tf32(kTcM, np), 0, mbar);
+  const bool done = tc_wait(mbar, 0, g.status,
+                            DCT_ERR_DEVICE_TIMEOUT, s, b);
+  if (done) {
+    const int row = (warp & 3) * 32 + lane;
+    const int32_t* rows = S.rows + S.rows_ptr[s];
+    const int lr = r0 + row;
+    const bool own = lr < ns;            // a pivot row of this supernode
+    float* dst = (row < nr) ? A + int64_t(rows[lr]) * g.k + j0 : nullptr;
+    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+      if (dst != nullptr) {
+        if (own) {
+          float cur[32];
+#pragma unroll
+          for (int c = 0; c < 32; ++c) cur[c] = (cb + c < kc) ? dst[cb + c] : 0.0f;
+#pragma unroll
+          for (int c = 0; c < 32; ++c)
+            if (cb + c < kc) dst[cb + c] = cur[c] - __uint_as_float(v[c]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 32; ++c)
+            if (cb + c < kc) atomicAdd(dst + cb + c, -__uint_as_float(v[c]));
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTcRhs);
+}
+
+// acc[c][j] += sum_r L[rows_r, c0 + c] x[rows_r, j] over the boundary rows
+// [ns, N) of front s (x gathered from A through the front's row list).
+template <typename T>
+__device__ void boundary_product(const T* F, int N, int ns, int c0, int w,
+                                 const int32_t* rows, const T* A, int k, int j0,
+                                 int rc, T* S1, T* S2, T (&acc)[4][4]) {
+  for (int i0 = ns; i0 < N; i0 += kLD) {
+    const int ni = min(kLD, N - i0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int r = idx % kLD, c = idx / kLD;
+      S1[r * kLD1 + c] = (r < ni && c < w) ? F[(i0 + r) + int64_t(c0 + c) * N] : T(0);
+    }
+    load_rhs(S2, A, k, j0, rc, ni, rows + i0, 0);
+    __syncthreads();
+    mm_tile(S1, S2, ni, w, acc);
+  }
+}
+
+// ------------------------------------------------------------ backward, small
+// one CTA: y -= L_B^T x_B ; x = D^{-T} y (to A)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bwd_small(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  T* Y = S2 + kLD * kLD;
+  const int s = g.tasks[blockIdx.x].s;
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int w = S.sn_first[s + 1] - first;
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  const T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  T acc[4][4];
+  zero_acc(acc);
+  boundary_product(F, N, w, 0, w, S.rows + S.rows_ptr[s], A, g.k, j0, rc, S1,
+                   S2, acc);
+  __syncthreads();
+  // Y = y - acc
+  load_rhs(Y, Bo, g.k, j0, rc, w, nullptr, first);
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Y[(ag + 16 * p) * kLD + jg + 16 * q] -= acc[p][q];
+  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s], w, true);
+  __syncthreads();
+  zero_acc(acc);
+  mm_tile(S1, Y, w, w, acc);
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ag + 16 * p, j = jg + 16 * q;
+      if (r < w && j < rc) A[int64_t(first + r) * g.k + j0 + j] = acc[p][q];
+    }
+}
+
+// ------------------------------------------------------------ backward gemm
+// large supernodes: y_p (B) -= L[boundary rows, panel p]^T x[boundary rows]
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bwd_gemm(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  const T* A = g.A + int64_t(b) * g.n * g.k;
+  T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  T acc[4][4];
+  zero_acc(acc);
+  boundary_product(F, N, ns, c0, w, S.rows + S.rows_ptr[s], A, g.k, j0, rc, S1,
+                   S2, acc);
+  T cur[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, j = jg + 16 * q;
+      cur[p][q] = (c < w && j < rc) ? Bo[int64_t(first + c0 + c) * g.k + j0 + j] : T(0);
+    }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, j = jg + 16 * q;
+      if (c < w && j < rc) Bo[int64_t(first + c0 + c) * g.k + j0 + j] = cur[p][q] - acc[p][q];
+    }
+}
+
+// ------------------------------------------------------------ backward step
+// large supernodes, panel p: x_p = D_p^{-T} y_p.  t0 == p: write x_p to A;
+// t0 = i < p: y_i (B) -= L[panel p rows, panel i cols]^T x_p.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bwd_step(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  T* X = S2 + kLD * kLD;
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s] + int64_t(tk.p) * kPanel * kPanel,
+            w, true);
+  load_rhs(S2, Bo, g.k, j0, rc, w, nullptr, first + c0);
+  __syncthreads();
+  T acc[4][4];
+  zero_acc(acc);
+  mm_tile(S1, S2, w, w, acc);
+  if (tk.t0 == tk.p) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = ag + 16 * p, j = jg + 16 * q;
+        if (r < w && j < rc) A[int64_t(first + c0 + r) * g.k + j0 + j] = acc[p][q];
+      }
     return;
   }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) X[(ag + 16 * p) * kLD + jg + 16 * q] = acc[p][q];
   const int ci0 = tk.t0 * kPanel;     // earlier panels are full width
-  for (int idx = threadIdx.x; idx < w * kPanel; idx += blockDim.x) {
-    const int r = idx % w, c = idx / w;
-    Lt[r + c * kPanel] = F[(c0 + r) + int64_t(ci0 + c) * N];
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+    const int r = idx % kLD, c = idx / kLD;
+    S1[r * kLD1 + c] = (r < w) ? F[(c0 + r) + int64_t(ci0 + c) * N] : T(0);
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < kPanel * rc; idx += blockDim.x) {
-    const int c = idx / rc, j = idx % rc;
-    T acc = T(0);
-    for (int r = 0; r < w; ++r) acc += Lt[r + c * kPanel] * Y[r * (kRhsChunk + 1) + j];
-    Bo[int64_t(first + ci0 + c) * k + j0 + j] -= acc;
-  }
+  zero_acc(acc);
+  mm_tile(S1, X, w, kLD, acc);
+  T cur[4][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, j = jg + 16 * q;
+      cur[p][q] = (j < rc) ? Bo[int64_t(first + ci0 + c) * g.k + j0 + j] : T(0);
+    }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, j = jg + 16 * q;
+      if (j < rc) Bo[int64_t(first + ci0 + c) * g.k + j0 + j] = cur[p][q] - acc[p][q];
+    }
 }
 
 // ------------------------------------------------------------ permutations
@@ -263,7 +565,7 @@ __global__ void k_convert(const TI* __restrict__ src, int64_t sstride, int64_t c
 
 // ------------------------------------------------------------ refinement
 // r = b - A x in float64 (permuted order), stored as float into the f32 work
-// buffer, with max|r| and max|b| folded into the status residual slots.
+// buffer, with max|r| and max|b| folded into the plan's residual words.
 __global__ void k_residual(DevSym S, const double* __restrict__ vals,
                            int64_t vals_stride, const double* __restrict__ b,
                            int64_t bstride, const double* __restrict__ x, int n,
@@ -314,57 +616,62 @@ inline dim3 grid1d(int64_t total, int ny) {
 
 template <typename T>
 cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
-  const int n = P->sym.n;
-  const int nchunk = (k + kRhsChunk - 1) / kRhsChunk;
-  const size_t step_smem =
-      sizeof(T) * (2 * kPanel * kPanel + kPanel * (kRhsChunk + 1));
-  const size_t gemm_smem = sizeof(T) * (kPanel * kPanel + kPanel * (kRhsChunk + 1));
-  cudaError_t e = cudaFuncSetAttribute(
-      k_fwd_step<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      static_cast<int>(step_smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_bwd_step<T>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(step_smem));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_bwd_gemm<T>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(gemm_smem));
-  if (e != cudaSuccess) return e;
-  const T* fronts = static_cast<const T*>(P->fronts);
-  const double nb = P->nbatch;
-  for (size_t li = 0; li < P->fwd.launches.size(); ++li) {
-    const Launch& L = P->fwd.launches[li];
-    if (L.count <= 0) continue;
-    if ((e = P->prof.begin(L.kind, P->fwd.flops[li] * k * nb,
-                           (P->fwd.bytes[li] + P->fwd.bytes_rhs[li] * k) * nb,
-                           st)) != cudaSuccess)
-      return e;
-    dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
-    k_fwd_step<T><<<grid, kThreads, step_smem, st>>>(
-        P->ds, P->fwd.d_tasks + L.first, fronts, P->front_stride, bufA, bufB, n,
-        k, nchunk);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = P->prof.end(st)) != cudaSuccess) return e;
+  const int nchunk = (k + kRC - 1) / kRC;
+  const size_t smem3 = sizeof(T) * (kLD1 * kLD + 2 * kLD * kLD);
+  cudaError_t e = cudaSuccess;
+  const void* kernels[] = {reinterpret_cast<const void*>(k_fwd_small<T>),
+                           reinterpret_cast<const void*>(k_fwd_step<T>),
+                           reinterpret_cast<const void*>(k_bwd_small<T>),
+                           reinterpret_cast<const void*>(k_bwd_gemm<T>),
+                           reinterpret_cast<const void*>(k_bwd_step<T>)};
+  for (const void* kf : kernels) {
+    e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem3));
+    if (e != cudaSuccess) return e;
   }
-  for (size_t li = 0; li < P->bwd.launches.size(); ++li) {
-    const Launch& L = P->bwd.launches[li];
-    if (L.count <= 0) continue;
-    if ((e = P->prof.begin(L.kind, P->bwd.flops[li] * k * nb,
-                           (P->bwd.bytes[li] + P->bwd.bytes_rhs[li] * k) * nb,
-                           st)) != cudaSuccess)
-      return e;
-    dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
-    if (L.kind == kBwdGemm)
-      k_bwd_gemm<T><<<grid, kThreads, gemm_smem, st>>>(
-          P->ds, P->bwd.d_tasks + L.first, fronts, P->front_stride, bufA, bufB,
-          n, k, nchunk);
-    else
-      k_bwd_step<T><<<grid, kThreads, step_smem, st>>>(
-          P->ds, P->bwd.d_tasks + L.first, fronts, P->front_stride, bufA, bufB,
-          n, k, nchunk);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = P->prof.end(st)) != cudaSuccess) return e;
+  SolveArgs<T> g{P->ds, nullptr, static_cast<const T*>(P->fronts), P->front_stride,
+                 static_cast<const T*>(P->dinv), P->d_dinv_off, P->dinv_stride,
+                 bufA, bufB, P->sym.n, k, nchunk, P->status};
+  if constexpr (sizeof(T) == 4) {
+    e = cudaFuncSetAttribute(k_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kFwdTcSmem));
+    if (e != cudaSuccess) return e;
+  }
+  const double nb = P->nbatch;
+  for (const Schedule* sc : {&P->fwd, &P->bwd}) {
+    for (size_t li = 0; li < sc->launches.size(); ++li) {
+      const Launch& L = sc->launches[li];
+      if (L.count <= 0) continue;
+      if ((e = P->prof.begin(L.kind, sc->flops[li] * k * nb,
+                             (sc->bytes[li] + sc->bytes_rhs[li] * k) * nb, st)) !=
+          cudaSuccess)
+        return e;
+      g.tasks = sc->d_tasks + L.first;
+      dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
+      if (L.kind == kFwdTc) {
+        if constexpr (sizeof(T) == 4) {
+          SolveArgs<float> gt = g;
+          gt.nchunk = (k + kTcRhs - 1) / kTcRhs;
+          dim3 gg(static_cast<unsigned>(L.count), P->nbatch * gt.nchunk);
+          k_fwd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
+        } else {
+          return cudaErrorInvalidValue;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = P->prof.end(st)) != cudaSuccess) return e;
+        continue;
+      }
+      switch (L.kind) {
+        case kFwdSmall: k_fwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kFwdStep: k_fwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kBwdSmall: k_bwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kBwdGemm: k_bwd_gemm<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kBwdStep: k_bwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;
+        default: return cudaErrorInvalidValue;
+      }
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = P->prof.end(st)) != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
 }

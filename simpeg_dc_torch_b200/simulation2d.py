@@ -66,7 +66,7 @@ class TorchDC2D:
     def __init__(self, mesh, survey, nky=12, device="cuda",
                  dtype=torch.float64, active_cells=None, val_inactive=None,
                  chunk=None, singularity_removal=False, rho_primary=None,
-                 quadrature=None, refine=None):
+                 quadrature=None, refine=None, refine_fields=None):
         if singularity_removal:
             raise NotImplementedError(
                 "singularity removal is not part of this implementation")
@@ -116,7 +116,7 @@ class TorchDC2D:
                                ops.sidx, self.device, precision,
                                coords=mesh.node_grid_index()
                                if hasattr(mesh, "node_grid_index") else None,
-                               refine=refine)
+                               refine=refine, refine_fields=refine_fields)
         self.solver = self._path.solver
         self.sidx = torch.as_tensor(ops.sidx, device=self.device)
         self.iD = torch.arange(self.nD, device=self.device)

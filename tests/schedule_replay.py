@@ -13,8 +13,9 @@ from __future__ import annotations
 import numpy as np
 
 PANEL = 64
-RHS_CHUNK = 32
-(SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, FWD, BWDGEMM, BWDSTEP) = range(8)
+UTILE = 64
+(SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, FWD, BWDGEMM, BWDSTEP, FWDSMALL,
+ BWDSMALL, PINV, FWDTC) = range(12)
 
 
 class Struct:
@@ -49,7 +50,14 @@ def _chol_lower(D):
     return D
 
 
-def _task_factor(S, kind, tk, fronts, vals, arg):
+def _factor_diag(S, F, s, c0, w, dinv):
+    L = _chol_lower(F[c0:c0 + w, c0:c0 + w])
+    blk = F[c0:c0 + w, c0:c0 + w]
+    blk[np.tril(np.ones((w, w), bool))] = L[np.tril(np.ones((w, w), bool))]
+    dinv[(s, c0 // PANEL)] = np.linalg.inv(L)
+
+
+def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE):
     s, p, t0, t1 = (int(v) for v in tk)
     N = int(S.front_n[s])
     ns = S.ns(s)
@@ -94,49 +102,59 @@ def _task_factor(S, kind, tk, fronts, vals, arg):
         c0 = p * PANEL
         w = min(PANEL, ns - c0)
         assert w > 0 and t0 >= 1
-        D = _chol_lower(F[c0:c0 + w, c0:c0 + w])
+        Di = dinv[(s, p)]           # stored when the diagonal was factored
         r0 = c0 + w + (t0 - 1) * PANEL
         nr = min(PANEL, N - r0)
         assert nr > 0
-        X = F[r0:r0 + nr, c0:c0 + w]
-        F[r0:r0 + nr, c0:c0 + w] = np.linalg.solve(D, X.T).T
+        F[r0:r0 + nr, c0:c0 + w] = F[r0:r0 + nr, c0:c0 + w] @ Di.T
     elif kind == LUPDATE:
         c0 = p * PANEL
         w = min(PANEL, ns - c0)
         base = c0 + w
         if t0 < 0:
-            F[c0:c0 + w, c0:c0 + w] = np.where(
-                np.tril(np.ones((w, w), bool)),
-                _chol_lower(F[c0:c0 + w, c0:c0 + w]), F[c0:c0 + w, c0:c0 + w])
+            _factor_diag(S, F, s, c0, w, dinv)
             return
-        ri, rj = base + t0 * PANEL, base + t1 * PANEL
+        ri, rj = base + t0 * utile, base + t1 * utile
         assert ri < N and rj < N and t0 >= t1
-        ni, nj = min(PANEL, N - ri), min(PANEL, N - rj)
+        ni, nj = min(utile, N - ri), min(utile, N - rj)
         F[ri:ri + ni, rj:rj + nj] -= (F[ri:ri + ni, c0:c0 + w]
                                       @ F[rj:rj + nj, c0:c0 + w].T)
+        if t0 == 0 and t1 == 0 and base < ns:
+            _factor_diag(S, F, s, base, min(PANEL, ns - base), dinv)
+    elif kind == PINV:
+        c0 = p * PANEL
+        w = min(PANEL, ns - c0)
+        dinv[(s, p)] = np.linalg.inv(np.tril(F[c0:c0 + w, c0:c0 + w]))
     else:
         raise AssertionError(f"unexpected kind {kind}")
 
 
 def replay_factor(sym, S, vals, dtype=0):
-    tasks, launches = sym.schedule(dtype, 0)
+    """Returns (fronts, dinv) with dinv[(s, p)] the stored panel inverses."""
     fronts = np.zeros(S.front_total)
-    for kind, lv, first, count, arg in launches:
-        chunk = tasks[first:first + count]
-        snap = fronts.copy()
-        for tk in chunk:
-            _task_factor(S, kind, tk, fronts, vals, arg)
-        fwd_result = fronts.copy()
-        fronts[:] = snap
-        for tk in chunk[::-1]:
-            _task_factor(S, kind, tk, fronts, vals, arg)
-        scale = max(1.0, np.abs(fwd_result).max())
-        assert np.abs(fronts - fwd_result).max() <= 1e-9 * scale, \
-            f"launch kind {kind} level {lv}: result depends on task order"
-    return fronts
+    dinv = {}
+    utile = UTILE if dtype == 0 else 128
+    for which in (0, 3):
+        tasks, launches = sym.schedule(dtype, which)
+        for kind, lv, first, count, arg in launches:
+            chunk = tasks[first:first + count]
+            snap, dsnap = fronts.copy(), dict(dinv)
+            for tk in chunk:
+                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
+            fwd_result, fwd_dinv = fronts.copy(), dict(dinv)
+            fronts[:], dinv = snap, dsnap
+            for tk in chunk[::-1]:
+                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
+            scale = max(1.0, np.abs(fwd_result).max())
+            assert np.abs(fronts - fwd_result).max() <= 1e-9 * scale, \
+                f"launch kind {kind} level {lv}: result depends on task order"
+            assert fwd_dinv.keys() == dinv.keys()
+    npanels = sum((S.ns(s) + PANEL - 1) // PANEL for s in range(S.nsuper))
+    assert len(dinv) == npanels, "a panel inverse was never stored"
+    return fronts, dinv
 
 
-def _task_solve(S, kind, tk, fronts, A, B):
+def _task_solve(S, kind, tk, fronts, A, B, dinv):
     s, p, t0, t1 = (int(v) for v in tk)
     N = int(S.front_n[s])
     ns = S.ns(s)
@@ -146,23 +164,37 @@ def _task_solve(S, kind, tk, fronts, A, B):
     w = min(PANEL, ns - c0)
     rows = S.rows[S.rows_ptr[s]:S.rows_ptr[s + 1]]
     assert rows.size == N
-    if kind == FWD:
-        D = np.tril(F[c0:c0 + w, c0:c0 + w])
-        y = np.linalg.solve(D, A[first + c0:first + c0 + w])
+    if kind == FWDSMALL:
+        assert ns <= PANEL and p == 0
+        y = dinv[(s, 0)] @ A[first:first + ns]
+        B[first:first + ns] = y
+        A[rows[ns:]] -= F[ns:, :ns] @ y
+    elif kind == BWDSMALL:
+        assert ns <= PANEL and p == 0
+        y = B[first:first + ns] - F[ns:, :ns].T @ A[rows[ns:]]
+        A[first:first + ns] = dinv[(s, 0)].T @ y
+    elif kind == FWD:
+        assert ns > PANEL
+        y = dinv[(s, p)] @ A[first + c0:first + c0 + w]
         if t0 == 0:
             B[first + c0:first + c0 + w] = y
             return
         r0 = c0 + w + (t0 - 1) * PANEL
-        nr = min(PANEL, N - r0)
-        assert nr > 0
-        upd = F[r0:r0 + nr, c0:c0 + w] @ y
-        A[rows[r0:r0 + nr]] -= upd
+        r1 = min(c0 + w + t1 * PANEL, N)
+        assert r0 < r1 <= N
+        A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
+    elif kind == FWDTC:
+        assert ns > PANEL
+        y = B[first + c0:first + c0 + w]          # written by the y launch
+        r0 = c0 + w + t0 * 128
+        r1 = min(r0 + 128, N)
+        assert r0 < r1
+        A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
     elif kind == BWDGEMM:
         xb = A[rows[ns:]]
         B[first + c0:first + c0 + w] -= F[ns:, c0:c0 + w].T @ xb
     elif kind == BWDSTEP:
-        D = np.tril(F[c0:c0 + w, c0:c0 + w])
-        x = np.linalg.solve(D.T, B[first + c0:first + c0 + w])
+        x = dinv[(s, p)].T @ B[first + c0:first + c0 + w]
         if t0 == p:
             A[first + c0:first + c0 + w] = x
             return
@@ -173,7 +205,7 @@ def _task_solve(S, kind, tk, fronts, A, B):
         raise AssertionError(f"unexpected kind {kind}")
 
 
-def replay_solve(sym, S, fronts, bp, dtype=0):
+def replay_solve(sym, S, fronts, bp, dinv, dtype=0):
     """bp: permuted rhs (n, k).  Returns the permuted solution."""
     A = np.array(bp, dtype=float, copy=True)
     B = np.zeros_like(A)
@@ -183,11 +215,11 @@ def replay_solve(sym, S, fronts, bp, dtype=0):
             chunk = tasks[first:first + count]
             sa, sb = A.copy(), B.copy()
             for tk in chunk:
-                _task_solve(S, kind, tk, fronts, A, B)
+                _task_solve(S, kind, tk, fronts, A, B, dinv)
             ra, rb = A.copy(), B.copy()
             A[:], B[:] = sa, sb
             for tk in chunk[::-1]:
-                _task_solve(S, kind, tk, fronts, A, B)
+                _task_solve(S, kind, tk, fronts, A, B, dinv)
             scale = max(1.0, np.abs(ra).max(), np.abs(rb).max())
             assert max(np.abs(A - ra).max(), np.abs(B - rb).max()) <= 1e-9 * scale, \
                 f"solve launch kind {kind} level {lv}: depends on task order"

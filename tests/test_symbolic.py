@@ -35,7 +35,7 @@ def laplacian(nx):
     return A
 
 
-def _check(A, coords, leaf, rhs):
+def _check(A, coords, leaf, rhs, dtype=0):
     sym = nat.Symbolic(A.indptr, A.indices, coords, leaf)
     S = Struct(sym)
     n = A.shape[0]
@@ -45,9 +45,9 @@ def _check(A, coords, leaf, rhs):
     assert S.sn_first[0] == 0 and S.sn_first[-1] == n
     par = S.sn_parent
     assert np.all((par == -1) | (par > np.arange(par.size)))
-    fronts = replay_factor(sym, S, A.data)
+    fronts, dinv = replay_factor(sym, S, A.data, dtype)
     bp = rhs[S.perm]
-    xp = replay_solve(sym, S, fronts, bp)
+    xp = replay_solve(sym, S, fronts, bp, dinv, dtype)
     x = np.empty_like(xp)
     x[S.perm] = xp
     xr = spla.spsolve(A.tocsc(), rhs)
@@ -65,12 +65,13 @@ def test_replay_2d_grid(coords):
     assert info["nnz_L"] < 0.2 * ops.nN ** 2
 
 
-@pytest.mark.parametrize("leaf", [16, 64])
-def test_replay_3d_grid_with_large_fronts(leaf):
+@pytest.mark.parametrize("leaf,dtype", [(16, 0), (64, 0), (64, 1)])
+def test_replay_3d_grid_with_large_fronts(leaf, dtype):
+    """dtype 1 replays the float32 plan's schedule (128-row tensor-core tiles)."""
     mesh, survey, m = syn.suite_case("3d-tensor")
     ops = nodal_operators(mesh, survey)
     A = ops.A(np.exp(-m))
-    err, info = _check(A, mesh.node_grid_index(), leaf, ops.q.toarray())
+    err, info = _check(A, mesh.node_grid_index(), leaf, ops.q.toarray(), dtype)
     assert err < 1e-12
     assert info["max_front"] > 160      # the multi-CTA front path is covered
 
@@ -108,7 +109,7 @@ def test_schedule_counts_are_consistent():
     ops = nodal_operators(mesh, survey)
     sym = nat.Symbolic(ops.crow, ops.col, mesh.node_grid_index(), 64)
     for dtype in (0, 1):
-        for which in (0, 1, 2):
+        for which in (0, 1, 2, 3):
             tasks, launches = sym.schedule(dtype, which)
             assert launches[:, 3].sum() == tasks.shape[0]
             assert np.all(np.diff(launches[:, 2]) >= 0)
