@@ -80,7 +80,7 @@ int dct_symbolic_get_array(const dct_symbolic* sym, const char* name,
 
 /* Host-side copy of the launch schedule a plan of this dtype would run
  * (which: 0 factorization, 1 forward, 2 backward substitution, 3 panel
- * inverses), for
+ * inverses, 4 supernode inverses), for
  * inspection and CPU-side replay in tests.  tasks: 4 int32 per task
  * (supernode, panel, t0, t1); launches: 5 int64 per launch (kind, level,
  * first task, task count, arg).  With null outputs only the counts are set. */
@@ -130,7 +130,9 @@ int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
  * (0 small fronts, 1 large scatter, 2 extend-add, 3 panel, 4 trailing
  * update, 5 forward step, 6 backward gemm, 7 backward step, 8 forward of
  * single-panel supernodes, 9 backward of single-panel supernodes, 10 panel
- * inverses, 11 forward row tiles on tensor cores), the summed
+ * inverses, 11 forward row tiles on tensor cores, 12 forward boundary rows,
+ * 13 forward boundary rows on tensor cores, 14-16 supernode-inverse steps,
+ * 17 forward inverse products, 18 backward inverse products), the summed
  * device milliseconds, the launch count and the algorithmic flops and bytes
  * of those launches; reset clears the counters. */
 int dct_plan_profile(dct_plan* plan, int32_t enable, int32_t reset);

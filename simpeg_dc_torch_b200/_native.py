@@ -226,7 +226,9 @@ class Plan:
 
     KINDS = ("small_front", "large_scatter", "extend_add", "panel_trsm",
              "trailing_update", "fwd_step", "bwd_gemm", "bwd_step",
-             "fwd_small", "bwd_small", "panel_inverse", "fwd_tc")
+             "fwd_small", "bwd_small", "panel_inverse", "fwd_tc", "fwd_bnd",
+             "fwd_bnd_tc", "linv_init", "linv_t", "linv_x", "fwd_linv",
+             "bwd_linv")
 
     def profile(self, enable, reset=True):
         check(lib().dct_plan_profile(self._h, int(bool(enable)), int(reset)),

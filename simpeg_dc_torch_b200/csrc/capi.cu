@@ -151,6 +151,19 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
         f += double(w) * w + 2 * nbd * w;
         bf += es * (w * (w + 1) / 2.0 + nbd * w);
         br += es * (2.0 * w + nbd);
+      } else if (l.kind == dct::kFwdLinv || l.kind == dct::kBwdLinv) {
+        const double nr = std::min(dct::kPanel, ns - t.t0 * dct::kPanel);
+        const double kk = l.kind == dct::kFwdLinv ? (t.t0 * dct::kPanel + nr)
+                                                   : (ns - t.t0 * dct::kPanel);
+        f += 2 * nr * kk;
+        bf += es * nr * kk;
+        br += es * (nr + kk);
+      } else if (l.kind == dct::kFwdBnd || l.kind == dct::kFwdBndTc) {
+        const int tile = l.kind == dct::kFwdBndTc ? 128 : dct::kPanel;
+        const double nr = std::min(tile, N - (ns + t.t0 * tile));
+        f += 2 * nr * ns;
+        bf += es * nr * ns;
+        br += es * (2 * nr + ns);
       } else if (l.kind == dct::kFwdTc) {
         const int r0 = c0 + w + t.t0 * 128;
         const double nr = std::min(128, N - r0);
@@ -269,85 +282,109 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile,
   }
 }
 
+// Forward and backward substitution schedules.  Per level of the assembly
+// tree: single-panel supernodes run one CTA each (kFwdSmall / kBwdSmall);
+// larger ones multiply by their precomputed inverse L_ss^{-1}
+// (kFwdLinv / kBwdLinv, 64-row tiles) and exchange with their boundary rows
+// once (kFwdBnd[Tc] after, kBwdGemm before).  A pass is a few launches per
+// level, independent of the supernodes' widths.
 void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
                            dct::Schedule* bwd) {
-  // float32 plans apply the row tiles below a panel on the tensor cores
-  // (128-row tiles, kFwdTc) after a launch that forms y_p (k_fwd_step, t0 = 0)
   const bool tc = dtype == DCT_F32;
   auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel; };
+  auto add = [](dct::Schedule* sc, int kind, int lv, auto&& fill) {
+    Launch l{kind, lv, int64_t(sc->tasks.size()), 0, 0};
+    fill(sc->tasks);
+    l.count = int64_t(sc->tasks.size()) - l.first;
+    if (l.count) sc->launches.push_back(l);
+  };
   for (int lv = 0; lv < S.nlevels; ++lv) {
-    Launch ls{dct::kFwdSmall, lv, int64_t(fwd->tasks.size()), 0, 0};
-    int max_panels = 0;
-    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-      int s = S.level_sn[q];
-      if (is_small(s)) fwd->tasks.push_back({s, 0, 0, 0});
-      else max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
-    }
-    ls.count = int64_t(fwd->tasks.size()) - ls.first;
-    if (ls.count) fwd->launches.push_back(ls);
-    for (int p = 0; p < max_panels; ++p) {
-      Launch l{dct::kFwdStep, lv, int64_t(fwd->tasks.size()), 0, p};
-      for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-        int s = S.level_sn[q];
+    const int q0 = S.level_ptr[lv], q1 = S.level_ptr[lv + 1];
+    add(fwd, dct::kFwdSmall, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q)
+        if (is_small(S.level_sn[q])) T.push_back({S.level_sn[q], 0, 0, 0});
+    });
+    add(fwd, dct::kFwdLinv, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q) {
+        const int s = S.level_sn[q];
         if (is_small(s)) continue;
-        int ns = S.ns(s), N = S.front_n[s];
-        int c0 = p * dct::kPanel;
-        if (c0 >= ns) continue;
-        int w = std::min(dct::kPanel, ns - c0);
-        int nt = ceil_div(N - c0 - w, dct::kPanel);
-        fwd->tasks.push_back({s, p, 0, 0});
-        if (!tc)
-          for (int t = 0; t < nt; t += dct::kRowGroup)
-            fwd->tasks.push_back({s, p, t + 1, std::min(nt, t + dct::kRowGroup)});
+        for (int t = 0; t * dct::kPanel < S.ns(s); ++t) T.push_back({s, 0, t, 0});
       }
-      l.count = int64_t(fwd->tasks.size()) - l.first;
-      fwd->launches.push_back(l);
-      if (tc) {
-        Launch lt{dct::kFwdTc, lv, int64_t(fwd->tasks.size()), 0, p};
-        for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-          int s = S.level_sn[q];
-          if (is_small(s)) continue;
-          int ns = S.ns(s), N = S.front_n[s];
-          int c0 = p * dct::kPanel;
-          if (c0 >= ns) continue;
-          int w = std::min(dct::kPanel, ns - c0);
-          int nt = ceil_div(N - c0 - w, 128);
-          for (int t = 0; t < nt; ++t) fwd->tasks.push_back({s, p, t, 0});
-        }
-        lt.count = int64_t(fwd->tasks.size()) - lt.first;
-        if (lt.count) fwd->launches.push_back(lt);
+    });
+    const int tile = tc ? 128 : dct::kPanel;
+    add(fwd, tc ? dct::kFwdBndTc : dct::kFwdBnd, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q) {
+        const int s = S.level_sn[q];
+        if (is_small(s)) continue;
+        for (int t = 0; t < ceil_div(S.nb(s), tile); ++t) T.push_back({s, 0, t, 0});
       }
-    }
+    });
   }
   for (int lv = S.nlevels - 1; lv >= 0; --lv) {
-    Launch ls{dct::kBwdSmall, lv, int64_t(bwd->tasks.size()), 0, 0};
-    int max_panels = 0;
-    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-      int s = S.level_sn[q];
-      if (is_small(s)) bwd->tasks.push_back({s, 0, 0, 0});
-      else max_panels = std::max(max_panels, ceil_div(S.ns(s), dct::kPanel));
-    }
-    ls.count = int64_t(bwd->tasks.size()) - ls.first;
-    if (ls.count) bwd->launches.push_back(ls);
-    if (max_panels == 0) continue;
-    Launch lg{dct::kBwdGemm, lv, int64_t(bwd->tasks.size()), 0, 0};
-    for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-      int s = S.level_sn[q];
-      if (is_small(s) || S.nb(s) == 0) continue;
-      int np = ceil_div(S.ns(s), dct::kPanel);
-      for (int p = 0; p < np; ++p) bwd->tasks.push_back({s, p, 0, 0});
-    }
-    lg.count = int64_t(bwd->tasks.size()) - lg.first;
-    if (lg.count) bwd->launches.push_back(lg);
-    for (int p = max_panels - 1; p >= 0; --p) {
-      Launch l{dct::kBwdStep, lv, int64_t(bwd->tasks.size()), 0, p};
-      for (int q = S.level_ptr[lv]; q < S.level_ptr[lv + 1]; ++q) {
-        int s = S.level_sn[q];
-        if (is_small(s) || p * dct::kPanel >= S.ns(s)) continue;
-        for (int i = 0; i <= p; ++i) bwd->tasks.push_back({s, p, i, 0});
+    const int q0 = S.level_ptr[lv], q1 = S.level_ptr[lv + 1];
+    add(bwd, dct::kBwdSmall, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q)
+        if (is_small(S.level_sn[q])) T.push_back({S.level_sn[q], 0, 0, 0});
+    });
+    add(bwd, dct::kBwdGemm, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q) {
+        const int s = S.level_sn[q];
+        if (is_small(s) || S.nb(s) == 0) continue;
+        for (int p = 0; p * dct::kPanel < S.ns(s); ++p) T.push_back({s, p, 0, 0});
       }
-      l.count = int64_t(bwd->tasks.size()) - l.first;
-      bwd->launches.push_back(l);
+    });
+    add(bwd, dct::kBwdLinv, lv, [&](std::vector<PanelTask>& T) {
+      for (int q = q0; q < q1; ++q) {
+        const int s = S.level_sn[q];
+        if (is_small(s)) continue;
+        for (int t = 0; t * dct::kPanel < S.ns(s); ++t) T.push_back({s, 0, t, 0});
+      }
+    });
+  }
+}
+
+// Supernode inverses L_ss^{-1} (ns > 64) by recursive doubling from the
+// 64-column panel inverses: with L = [[A, 0], [C, D]] over blocks of h and
+// h' <= h columns, L^{-1} = [[A^{-1}, 0], [-D^{-1} C A^{-1}, D^{-1}]].  Level h
+// runs two launches over every pair of blocks: T = C A^{-1}, then
+// X = -D^{-1} T, on 64 x 64 output tiles (t0 = tile row, t1 = tile column,
+// p = pair index, launch arg = h).  Offsets: ns^2 elements per supernode.
+void build_linv_schedule(const dct::Symbolic& S, dct::Schedule* sc,
+                         std::vector<int64_t>* off, int64_t* total) {
+  off->assign(S.nsuper, -1);
+  int64_t acc = 0;
+  int max_ns = 0;
+  for (int s = 0; s < S.nsuper; ++s) {
+    const int ns = S.ns(s);
+    if (ns <= dct::kPanel) continue;
+    (*off)[s] = acc;
+    acc += int64_t(ns) * ns;
+    max_ns = std::max(max_ns, ns);
+  }
+  *total = acc;
+  {
+    Launch l{dct::kLinvInit, 0, int64_t(sc->tasks.size()), 0, 0};
+    for (int s = 0; s < S.nsuper; ++s)
+      if (S.ns(s) > dct::kPanel)
+        for (int p = 0; p * dct::kPanel < S.ns(s); ++p) sc->tasks.push_back({s, p, 0, 0});
+    l.count = int64_t(sc->tasks.size()) - l.first;
+    if (l.count) sc->launches.push_back(l);
+  }
+  for (int h = dct::kPanel; h < max_ns; h *= 2) {
+    for (int kind : {int(dct::kLinvT), int(dct::kLinvX)}) {
+      Launch l{kind, 0, int64_t(sc->tasks.size()), 0, h};
+      for (int s = 0; s < S.nsuper; ++s) {
+        const int ns = S.ns(s);
+        if (ns <= dct::kPanel) continue;
+        for (int i = 0; 2 * i * h + h < ns; ++i) {
+          const int d0 = 2 * i * h + h;
+          const int hd = std::min(h, ns - d0);
+          for (int r = 0; r < ceil_div(hd, dct::kPanel); ++r)
+            for (int c = 0; c < h / dct::kPanel; ++c) sc->tasks.push_back({s, i, r, c});
+        }
+      }
+      l.count = int64_t(sc->tasks.size()) - l.first;
+      if (l.count) sc->launches.push_back(l);
     }
   }
 }
@@ -534,7 +571,7 @@ int dct_symbolic_get_array(const dct_symbolic* h, const char* name, void* dst,
 int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t which,
                               int32_t* tasks, int64_t* ntasks, int64_t* launches,
                               int64_t* nlaunches) {
-  if (!h || !ntasks || !nlaunches || which < 0 || which > 3 ||
+  if (!h || !ntasks || !nlaunches || which < 0 || which > 4 ||
       (dtype != DCT_F64 && dtype != DCT_F32))
     return fail(DCT_ERR_ARG, "bad arguments");
   dct::Schedule f, fw, bw, iv;
@@ -544,7 +581,12 @@ int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t whic
   std::vector<int64_t> off;
   int64_t tot = 0;
   build_inverse_schedule(h->sym, small_max, &iv, &off, &tot);
-  const dct::Schedule& sc = which == 0 ? f : (which == 1 ? fw : (which == 2 ? bw : iv));
+  dct::Schedule lv;
+  std::vector<int64_t> loff;
+  int64_t ltot = 0;
+  build_linv_schedule(h->sym, &lv, &loff, &ltot);
+  const dct::Schedule& sc =
+      which == 0 ? f : (which == 1 ? fw : (which == 2 ? bw : (which == 3 ? iv : lv)));
   const int64_t nt = int64_t(sc.tasks.size()), nl = int64_t(sc.launches.size());
   if (tasks) {
     if (*ntasks < nt) return fail(DCT_ERR_ARG, "task buffer too small");
@@ -625,11 +667,19 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
     if ((rc = upload(P, dinv_off, &d))) return bail(rc);
     P->d_dinv_off = d;
   }
+  std::vector<int64_t> linv_off;
+  build_linv_schedule(S, &P->linv_sched, &linv_off, &P->linv_stride);
+  {
+    const int64_t* d = nullptr;
+    if ((rc = upload(P, linv_off, &d))) return bail(rc);
+    P->d_linv_off = d;
+  }
   account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype));
   account_solve(S, &P->fwd, double(esize(dtype)));
   account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||
-      (rc = upload_schedule(P, &P->bwd)) || (rc = upload_schedule(P, &P->inv)))
+      (rc = upload_schedule(P, &P->bwd)) || (rc = upload_schedule(P, &P->inv)) ||
+      (rc = upload_schedule(P, &P->linv_sched)))
     return bail(rc);
   const size_t es = esize(dtype);
   P->front_stride = S.front_total;
@@ -638,6 +688,10 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
   if ((rc = alloc(P, es * S.front_total * nbatch, &P->fronts, "front storage")))
     return bail(rc);
   if ((rc = alloc(P, es * P->dinv_stride * nbatch, &P->dinv, "panel inverses")))
+    return bail(rc);
+  if ((rc = alloc(P, es * P->linv_stride * nbatch, &P->linv, "supernode inverses")))
+    return bail(rc);
+  if ((rc = alloc(P, es * P->linv_stride * nbatch, &P->ltmp, "inverse products")))
     return bail(rc);
   if ((rc = alloc(P, es * work, &P->bufA, "work buffer A"))) return bail(rc);
   if ((rc = alloc(P, es * work, &P->bufB, "work buffer B"))) return bail(rc);

@@ -52,6 +52,13 @@ enum LaunchKind : int {
   kBwdSmall,         // backward substitution of single-panel supernodes
   kPanelInverse,     // inverses of the factored diagonal blocks
   kFwdTc,            // forward row-tile updates on tensor cores (float32)
+  kFwdBnd,           // forward boundary-row update of a supernode (float64)
+  kFwdBndTc,         // the same on tensor cores (float32)
+  kLinvInit,         // supernode inverses: diagonal 64-blocks from the panels
+  kLinvT,            // supernode inverses, doubling step T = C A^{-1}
+  kLinvX,            // supernode inverses, doubling step X = -D^{-1} T
+  kFwdLinv,          // forward: y_s = L_ss^{-1} b_s for large supernodes
+  kBwdLinv,          // backward: x_s = L_ss^{-T} y_s for large supernodes
   kNumKinds
 };
 
@@ -113,6 +120,11 @@ struct dct_plan {
   void* dinv = nullptr;            // nbatch * dinv_stride elements of dtype
   int64_t dinv_stride = 0;         // per system: sum over panels of w^2
   const int64_t* d_dinv_off = nullptr;   // per supernode, first panel inverse
+  dct::Schedule linv_sched;        // supernode-inverse doubling launches
+  void* linv = nullptr;            // nbatch * linv_stride: L_ss^{-1}, ns x ns (ld ns)
+  void* ltmp = nullptr;            // same size: doubling-step products
+  int64_t linv_stride = 0;
+  const int64_t* d_linv_off = nullptr;   // per supernode (-1 for one-panel ones)
   void* bufA = nullptr;            // dtype, nbatch*n*max_rhs (work buffer A)
   void* bufB = nullptr;            // dtype, nbatch*n*max_rhs (work buffer B)
   double* x64 = nullptr;           // f32 plans: refined solution (dct_solve)

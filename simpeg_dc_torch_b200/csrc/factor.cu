@@ -498,6 +498,160 @@ k_panel_inverse(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
   }
 }
 
+// ------------------------------------------------------------ supernode inverses
+// L_ss^{-1} (ns x ns, column-major, ld ns) of every supernode wider than one
+// panel, by recursive doubling from the panel inverses (see the schedule in
+// capi.cu).  Blocks of 64 x 64 tiles; K loops skip the zero upper blocks.
+struct LinvArgs {
+  DevSym S;
+  const PanelTask* tasks;
+  int64_t front_stride;
+  const int64_t* dinv_off;
+  int64_t dinv_stride;
+  const int64_t* linv_off;
+  int64_t linv_stride;
+  int h;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_linv_init(LinvArgs g, const T* dinv, T* linv) {
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s;
+  const int ns = g.S.sn_first[s + 1] - g.S.sn_first[s];
+  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
+  const T* Di = dinv + int64_t(b) * g.dinv_stride + g.dinv_off[s] + int64_t(tk.p) * kPanel * kPanel;
+  T* X = linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+    const int r = idx % w, c = idx / w;
+    X[(c0 + r) + int64_t(c0 + c) * ns] = Di[r + c * w];
+  }
+}
+
+// T[d-block, a-block] = C A^{-1}: C = L[d0.., a0..] (front rows), A^{-1} the
+// top block's inverse.  out tile (rt, ct): rows d0 + 64 rt, cols a0 + 64 ct.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_linv_t(LinvArgs g, const T* fronts, const T* linv, T* ltmp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);       // [k][c], ld 65: A^{-1}[k, c]
+  T* S2 = S1 + (kPanel + 1) * kPanel;           // [k][r], ld 64: C[r, k]
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s, h = g.h;
+  const DevSym& S = g.S;
+  const int N = S.front_n[s];
+  const int ns = S.sn_first[s + 1] - S.sn_first[s];
+  const int a0 = 2 * tk.p * h, d0 = a0 + h;
+  const int hd = min(h, ns - d0);
+  const int r0 = tk.t0 * kPanel, cc0 = tk.t1 * kPanel;
+  const int nr = min(kPanel, hd - r0);
+  const T* F = fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  const T* X = linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+  T* Tt = ltmp + int64_t(b) * g.linv_stride + g.linv_off[s];
+  T acc[4][4];
+  zero_acc(acc);
+  for (int k0 = cc0; k0 < h; k0 += kPanel) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+      const int q = idx % kPanel, c = idx / kPanel;   // q: k index (contiguous)
+      S1[q * (kPanel + 1) + c] = X[(a0 + k0 + q) + int64_t(a0 + cc0 + c) * ns];
+      const int r = idx % kPanel, kk = idx / kPanel;
+      S2[kk * kPanel + r] = (r < nr) ? F[(d0 + r0 + r) + int64_t(a0 + k0 + kk) * N] : T(0);
+    }
+    __syncthreads();
+    mm64<T, kPanel + 1, kPanel>(S1, S2, kPanel, kPanel, acc);   // acc[c][r]
+  }
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, r = jg + 16 * q;
+      if (r < nr) Tt[(d0 + r0 + r) + int64_t(a0 + cc0 + c) * ns] = acc[p][q];
+    }
+}
+
+// X[d-block, a-block] = -D^{-1} T with D^{-1} the bottom block's inverse.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_linv_x(LinvArgs g, const T* ltmp, T* linv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);       // [k][c], ld 65: T[k, c]
+  T* S2 = S1 + (kPanel + 1) * kPanel;           // [k][r], ld 64: D^{-1}[r, k]
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s, h = g.h;
+  const int ns = g.S.sn_first[s + 1] - g.S.sn_first[s];
+  const int a0 = 2 * tk.p * h, d0 = a0 + h;
+  const int hd = min(h, ns - d0);
+  const int r0 = tk.t0 * kPanel, cc0 = tk.t1 * kPanel;
+  const int nr = min(kPanel, hd - r0);
+  T* X = linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+  const T* Tt = ltmp + int64_t(b) * g.linv_stride + g.linv_off[s];
+  T acc[4][4];
+  zero_acc(acc);
+  for (int k0 = 0; k0 <= r0; k0 += kPanel) {
+    const int kw = min(kPanel, hd - k0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+      const int q = idx % kPanel, c = idx / kPanel;
+      S1[q * (kPanel + 1) + c] =
+          (q < kw) ? Tt[(d0 + k0 + q) + int64_t(a0 + cc0 + c) * ns] : T(0);
+      const int r = idx % kPanel, kk = idx / kPanel;
+      S2[kk * kPanel + r] =
+          (r < nr && kk < kw) ? X[(d0 + r0 + r) + int64_t(d0 + k0 + kk) * ns] : T(0);
+    }
+    __syncthreads();
+    mm64<T, kPanel + 1, kPanel>(S1, S2, kw, kPanel, acc);
+  }
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = ag + 16 * p, r = jg + 16 * q;
+      if (r < nr) X[(d0 + r0 + r) + int64_t(a0 + cc0 + c) * ns] = -acc[p][q];
+    }
+}
+
+template <typename T>
+cudaError_t run_linv(dct_plan* P, cudaStream_t st) {
+  const int nb = P->nbatch;
+  const size_t smem = sizeof(T) * ((kPanel + 1) * kPanel + kPanel * kPanel);
+  cudaError_t e = cudaFuncSetAttribute(k_linv_t<T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_linv_x<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  LinvArgs g{P->ds, nullptr, P->front_stride, P->d_dinv_off, P->dinv_stride,
+             P->d_linv_off, P->linv_stride, 0};
+  for (size_t li = 0; li < P->linv_sched.launches.size(); ++li) {
+    const Launch& L = P->linv_sched.launches[li];
+    if (L.count <= 0) continue;
+    if ((e = P->prof.begin(L.kind, 0.0, 0.0, st)) != cudaSuccess) return e;
+    g.tasks = P->linv_sched.d_tasks + L.first;
+    g.h = L.arg;
+    dim3 grid(static_cast<unsigned>(L.count), nb);
+    if (L.kind == kLinvInit)
+      k_linv_init<T><<<grid, kThreads, 0, st>>>(g, static_cast<const T*>(P->dinv),
+                                               static_cast<T*>(P->linv));
+    else if (L.kind == kLinvT)
+      k_linv_t<T><<<grid, kThreads, smem, st>>>(g, static_cast<const T*>(P->fronts),
+                                               static_cast<const T*>(P->linv),
+                                               static_cast<T*>(P->ltmp));
+    else
+      k_linv_x<T><<<grid, kThreads, smem, st>>>(g, static_cast<const T*>(P->ltmp),
+                                               static_cast<T*>(P->linv));
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = P->prof.end(st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                         int64_t vals_stride, cudaStream_t st) {
@@ -599,7 +753,7 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
     e = P->prof.end(st);
     if (e != cudaSuccess) return e;
   }
-  return cudaSuccess;
+  return run_linv<T>(P, st);
 }
 
 }  // namespace

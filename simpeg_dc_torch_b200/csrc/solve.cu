@@ -89,6 +89,9 @@ struct SolveArgs {
   T* B;
   int n, k, nchunk;
   int* status;
+  const T* linv;
+  const int64_t* linv_off;
+  int64_t linv_stride;
 };
 
 // ------------------------------------------------------------ forward, small
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_step(SolveArgs<T> g) {
   const int32_t* rows = S.rows + S.rows_ptr[s];
   for (int t = tk.t0 - 1; t < tk.t1; ++t) {
     const int r0 = c0 + w + t * kLD;
-    const int nr = min(kLD, N - r0);
+    const int nr = min(kLD, ns - r0);   // own rows only; boundary rows: k_fwd_bnd
     __syncthreads();
     for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
       const int r = idx % kLD, c = idx / kLD;
@@ -261,12 +264,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_fwd_tc(SolveArgs<float> g) {
   const int ns = S.sn_first[s + 1] - first;
   const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
   const int r0 = c0 + w + tk.t0 * kTcM;
-  const int nr = min(kTcM, N - r0);
+  const int nr = min(kTcM, ns - r0);   // own rows only; boundary rows: k_fwd_bnd_tc
   const float* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
   float* A = g.A + int64_t(b) * g.n * g.k;
   const float* Bo = g.B + int64_t(b) * g.n * g.k;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nwarps = blockDim.x >> 5;
 
   if (warp == 0) tmem_alloc(tmem_slot, kTcRhs);
   if (tid == 0) mbar_init(mbar);
@@ -349,6 +351,242 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_fwd_tc(SolveArgs<float> g) {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kTcRhs);
+}
+
+// ------------------------------------------------------------ forward, boundary
+// large supernodes, after all of their panel steps: the 64-row tile t of the
+// boundary rows [ns, N) receives -L[tile, 0:ns] y_s (y_s = all panels, in B),
+// accumulated over the panels before one atomic update per element.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fwd_bnd(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);
+  T* S2 = S1 + kLD1 * kLD;
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int r0 = ns + tk.t0 * kLD;
+  const int nr = min(kLD, N - r0);
+  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  const T* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+  T acc[4][4];
+  zero_acc(acc);
+  for (int c0 = 0; c0 < ns; c0 += kPanel) {
+    const int w = min(kPanel, ns - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int r = idx % kLD, c = idx / kLD;
+      S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c0 + c) * N] : T(0);
+    }
+    load_rhs(S2, Bo, g.k, j0, rc, w, nullptr, first + c0);
+    __syncthreads();
+    mm_tile(S1, S2, w, nr, acc);
+  }
+  const int32_t* rows = S.rows + S.rows_ptr[s];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    const int r = ag + 16 * p;
+    if (r >= nr) continue;
+    T* dst = A + int64_t(rows[r0 + r]) * g.k + j0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = jg + 16 * q;
+      if (j < rc) atomic_sub(dst + j, acc[p][q]);
+    }
+  }
+}
+
+// float32: the same boundary update on the tensor cores, 128 rows per CTA,
+// all right-hand sides (<= 256) per MMA, K = ns in steps of one panel with
+// the accumulator kept in TMEM.
+__global__ void __launch_bounds__(kTcThreads, 1) k_fwd_bnd_tc(SolveArgs<float> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char* Ahi = smem_raw;
+  unsigned char* Alo = Ahi + kTcOperandBytes;
+  unsigned char* Bhi = Alo + kTcOperandBytes;
+  unsigned char* Blo = Bhi + kTcRhsBytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcRhsBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kTcRhs;
+  const int kc = min(kTcRhs, g.k - j0);
+  const int np = (kc + 15) & ~15;
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int r0 = ns + tk.t0 * kTcM;
+  const int nr = min(kTcM, N - r0);
+  const float* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+  float* A = g.A + int64_t(b) * g.n * g.k;
+  const float* Bo = g.B + int64_t(b) * g.n * g.k;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int kWarps = kTcThreads / 32;
+  if (warp == 0) tmem_alloc(tmem_slot, kTcRhs);
+  if (tid == 0) mbar_init(mbar);
+  __syncthreads();
+  const uint32_t idesc = umma_idesc_tf32(kTcM, np);
+  bool ok = true;
+  int phase = 0;
+  for (int c0 = 0; c0 < ns && ok; c0 += kPanel, ++phase) {
+    const int w = min(kPanel, ns - c0);
+    {
+      constexpr int kPer = (kTcM / 8) * 16 / kWarps;
+      const int m_lo = lane >> 2, k_lo = lane & 3;
+      float v[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int cm = warp + u * kWarps;
+        const int m = (cm % (kTcM / 8)) * 8 + m_lo, kq = (cm / (kTcM / 8)) * 4 + k_lo;
+        v[u] = (m < nr && kq < w) ? F[(r0 + m) + int64_t(c0 + kq) * N] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int cm = warp + u * kWarps;
+        tc_store_split(Ahi, Alo,
+                       (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
+                       v[u]);
+      }
+    }
+    {
+      const int ncm = (np / 8) * 16;
+      const int j_lo = lane >> 2, k_lo = lane & 3;
+      for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
+        float v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int cm = c0m + warp + u * kWarps;
+          const int j = (cm % (np / 8)) * 8 + j_lo, kq = (cm / (np / 8)) * 4 + k_lo;
+          v[u] = (cm < ncm && j < kc && kq < w)
+                     ? Bo[int64_t(first + c0 + kq) * g.k + j0 + j] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int cm = c0m + warp + u * kWarps;
+          if (cm < ncm)
+            tc_store_split(Bhi, Blo,
+                           (cm % (np / 8)) * kTcSBO + (cm / (np / 8)) * kTcLBO + lane * 4,
+                           v[u]);
+        }
+      }
+    }
+    tc_publish_smem();
+    const uint32_t tmem = *tmem_slot;
+    if (tid == 0)
+      umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
+                  (w + 7) / 8, idesc, c0 > 0 ? 1u : 0u, mbar);
+    // the operands may be overwritten only after these MMAs completed
+    ok = tc_wait(mbar, uint32_t(phase & 1), g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
+  }
+  const uint32_t tmem = *tmem_slot;
+  if (ok) {
+    const int row = (warp & 3) * 32 + lane;
+    const int32_t* rows = S.rows + S.rows_ptr[s];
+    float* dst = (row < nr) ? A + int64_t(rows[r0 + row]) * g.k + j0 : nullptr;
+    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+      if (dst != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+          if (cb + c < kc) atomicAdd(dst + cb + c, -__uint_as_float(v[c]));
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTcRhs);
+}
+
+// ------------------------------------------------------------ inverse products
+// large supernodes: y_s = L_ss^{-1} b_s, 64-row tile t0 per CTA (B <- A rows)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_fwd_linv(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[a, k]
+  T* S2 = S1 + kLD1 * kLD;                  // [k][j]: b[k, j]
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int r0 = tk.t0 * kLD, nr = min(kLD, ns - r0);
+  const T* X = g.linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+  const T* A = g.A + int64_t(b) * g.n * g.k;
+  T* Bo = g.B + int64_t(b) * g.n * g.k;
+  T acc[4][4];
+  zero_acc(acc);
+  for (int k0 = 0; k0 <= r0; k0 += kLD) {
+    const int kw = min(kLD, ns - k0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int a = idx % kLD, kk = idx / kLD;
+      S1[kk * kLD1 + a] = (a < nr && kk < kw) ? X[(r0 + a) + int64_t(k0 + kk) * ns] : T(0);
+    }
+    load_rhs(S2, A, g.k, j0, rc, kw, nullptr, first + k0);
+    __syncthreads();
+    mm_tile(S1, S2, kw, nr, acc);
+  }
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ag + 16 * p, j = jg + 16 * q;
+      if (r < nr && j < rc) Bo[int64_t(first + r0 + r) * g.k + j0 + j] = acc[p][q];
+    }
+}
+
+// large supernodes: x_s = L_ss^{-T} y_s, 64-row tile t0 per CTA (A <- B rows)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_bwd_linv(SolveArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[k, a]
+  T* S2 = S1 + kLD1 * kLD;                  // [k][j]: y[k, j]
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const int rc = min(kRC, g.k - j0);
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int r0 = tk.t0 * kLD, nr = min(kLD, ns - r0);
+  const T* X = g.linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+  T* A = g.A + int64_t(b) * g.n * g.k;
+  const T* Bo = g.B + int64_t(b) * g.n * g.k;
+  T acc[4][4];
+  zero_acc(acc);
+  for (int k0 = r0; k0 < ns; k0 += kLD) {
+    const int kw = min(kLD, ns - k0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+      const int kk = idx % kLD, a = idx / kLD;
+      S1[kk * kLD1 + a] = (a < nr && kk < kw) ? X[(k0 + kk) + int64_t(r0 + a) * ns] : T(0);
+    }
+    load_rhs(S2, Bo, g.k, j0, rc, kw, nullptr, first + k0);
+    __syncthreads();
+    mm_tile(S1, S2, kw, nr, acc);
+  }
+  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int r = ag + 16 * p, j = jg + 16 * q;
+      if (r < nr && j < rc) A[int64_t(first + r0 + r) * g.k + j0 + j] = acc[p][q];
+    }
 }
 
 // acc[c][j] += sum_r L[rows_r, c0 + c] x[rows_r, j] over the boundary rows
@@ -620,6 +858,9 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
   const size_t smem3 = sizeof(T) * (kLD1 * kLD + 2 * kLD * kLD);
   cudaError_t e = cudaSuccess;
   const void* kernels[] = {reinterpret_cast<const void*>(k_fwd_small<T>),
+                           reinterpret_cast<const void*>(k_fwd_bnd<T>),
+                           reinterpret_cast<const void*>(k_fwd_linv<T>),
+                           reinterpret_cast<const void*>(k_bwd_linv<T>),
                            reinterpret_cast<const void*>(k_fwd_step<T>),
                            reinterpret_cast<const void*>(k_bwd_small<T>),
                            reinterpret_cast<const void*>(k_bwd_gemm<T>),
@@ -631,10 +872,14 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
   }
   SolveArgs<T> g{P->ds, nullptr, static_cast<const T*>(P->fronts), P->front_stride,
                  static_cast<const T*>(P->dinv), P->d_dinv_off, P->dinv_stride,
-                 bufA, bufB, P->sym.n, k, nchunk, P->status};
+                 bufA, bufB, P->sym.n, k, nchunk, P->status,
+                 static_cast<const T*>(P->linv), P->d_linv_off, P->linv_stride};
   if constexpr (sizeof(T) == 4) {
     e = cudaFuncSetAttribute(k_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(kFwdTcSmem));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_fwd_bnd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kFwdTcSmem));
     if (e != cudaSuccess) return e;
   }
   const double nb = P->nbatch;
@@ -648,12 +893,13 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
         return e;
       g.tasks = sc->d_tasks + L.first;
       dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
-      if (L.kind == kFwdTc) {
+      if (L.kind == kFwdTc || L.kind == kFwdBndTc) {
         if constexpr (sizeof(T) == 4) {
           SolveArgs<float> gt = g;
           gt.nchunk = (k + kTcRhs - 1) / kTcRhs;
           dim3 gg(static_cast<unsigned>(L.count), P->nbatch * gt.nchunk);
-          k_fwd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
+          if (L.kind == kFwdTc) k_fwd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
+          else k_fwd_bnd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
         } else {
           return cudaErrorInvalidValue;
         }
@@ -664,6 +910,9 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
       switch (L.kind) {
         case kFwdSmall: k_fwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kFwdStep: k_fwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kFwdBnd: k_fwd_bnd<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kFwdLinv: k_fwd_linv<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kBwdLinv: k_bwd_linv<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdSmall: k_bwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdGemm: k_bwd_gemm<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdStep: k_bwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;

@@ -15,7 +15,8 @@ import numpy as np
 PANEL = 64
 UTILE = 64
 (SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, FWD, BWDGEMM, BWDSTEP, FWDSMALL,
- BWDSMALL, PINV, FWDTC) = range(12)
+ BWDSMALL, PINV, FWDTC, FWDBND, FWDBNDTC, LINVINIT, LINVT, LINVX, FWDLINV,
+ BWDLINV) = range(19)
 
 
 class Struct:
@@ -125,6 +126,27 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE):
         c0 = p * PANEL
         w = min(PANEL, ns - c0)
         dinv[(s, p)] = np.linalg.inv(np.tril(F[c0:c0 + w, c0:c0 + w]))
+    elif kind == LINVINIT:
+        assert ns > PANEL
+        c0 = p * PANEL
+        w = min(PANEL, ns - c0)
+        dinv[("linv", s)][c0:c0 + w, c0:c0 + w] = dinv[(s, p)]
+    elif kind in (LINVT, LINVX):
+        # supernode inverse by doubling: pair p of blocks of h = arg columns
+        h = arg
+        X, Tt = dinv[("linv", s)], dinv[("ltmp", s)]
+        a0 = 2 * p * h
+        d0 = a0 + h
+        hd = min(h, ns - d0)
+        r0, cc0 = t0 * PANEL, t1 * PANEL
+        nr = min(PANEL, hd - r0)
+        assert hd > 0 and nr > 0 and cc0 + PANEL <= h
+        rs = slice(d0 + r0, d0 + r0 + nr)
+        cs = slice(a0 + cc0, a0 + cc0 + PANEL)
+        if kind == LINVT:
+            Tt[rs, cs] = F[rs, a0 + cc0:a0 + h] @ X[a0 + cc0:a0 + h, cs]
+        else:
+            X[rs, cs] = -X[rs, d0:d0 + r0 + nr] @ Tt[d0:d0 + r0 + nr, cs]
     else:
         raise AssertionError(f"unexpected kind {kind}")
 
@@ -133,15 +155,25 @@ def replay_factor(sym, S, vals, dtype=0):
     """Returns (fronts, dinv) with dinv[(s, p)] the stored panel inverses."""
     fronts = np.zeros(S.front_total)
     dinv = {}
+    # supernode inverses and their scratch start as NaN: a read of an entry
+    # that no earlier launch wrote poisons the result
+    for s in range(S.nsuper):
+        if S.ns(s) > PANEL:
+            dinv[("linv", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
+            dinv[("ltmp", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
     utile = UTILE if dtype == 0 else 128
-    for which in (0, 3):
+
+    def snapshot(d):
+        return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+
+    for which in (0, 3, 4):
         tasks, launches = sym.schedule(dtype, which)
         for kind, lv, first, count, arg in launches:
             chunk = tasks[first:first + count]
-            snap, dsnap = fronts.copy(), dict(dinv)
+            snap, dsnap = fronts.copy(), snapshot(dinv)
             for tk in chunk:
                 _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
-            fwd_result, fwd_dinv = fronts.copy(), dict(dinv)
+            fwd_result, fwd_dinv = fronts.copy(), snapshot(dinv)
             fronts[:], dinv = snap, dsnap
             for tk in chunk[::-1]:
                 _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
@@ -149,8 +181,21 @@ def replay_factor(sym, S, vals, dtype=0):
             assert np.abs(fronts - fwd_result).max() <= 1e-9 * scale, \
                 f"launch kind {kind} level {lv}: result depends on task order"
             assert fwd_dinv.keys() == dinv.keys()
+            for key, v in dinv.items():
+                u = fwd_dinv[key]
+                assert np.array_equal(np.isnan(u), np.isnan(v))
+                ok = ~np.isnan(u)
+                assert np.abs(u[ok] - v[ok]).max(initial=0.0) <= 1e-9 * max(
+                    1.0, np.abs(u[ok]).max(initial=0.0)), \
+                    f"launch kind {kind}: {key} depends on task order"
     npanels = sum((S.ns(s) + PANEL - 1) // PANEL for s in range(S.nsuper))
-    assert len(dinv) == npanels, "a panel inverse was never stored"
+    assert len([k for k in dinv if k[0] not in ("linv", "ltmp")]) == npanels, \
+        "a panel inverse was never stored"
+    for s in range(S.nsuper):
+        if S.ns(s) > PANEL:
+            X = dinv[("linv", s)]
+            low = np.tril(np.ones_like(X, dtype=bool))
+            assert not np.isnan(X[low]).any(), f"supernode {s}: inverse incomplete"
     return fronts, dinv
 
 
@@ -180,16 +225,36 @@ def _task_solve(S, kind, tk, fronts, A, B, dinv):
             B[first + c0:first + c0 + w] = y
             return
         r0 = c0 + w + (t0 - 1) * PANEL
-        r1 = min(c0 + w + t1 * PANEL, N)
-        assert r0 < r1 <= N
+        r1 = min(c0 + w + t1 * PANEL, ns)
+        assert r0 < r1 <= ns
         A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
+    elif kind in (FWDBND, FWDBNDTC):
+        tile = 128 if kind == FWDBNDTC else PANEL
+        r0 = ns + t0 * tile
+        r1 = min(r0 + tile, N)
+        assert ns < r0 + 1 <= r1
+        A[rows[r0:r1]] -= F[r0:r1, :ns] @ B[first:first + ns]
     elif kind == FWDTC:
         assert ns > PANEL
         y = B[first + c0:first + c0 + w]          # written by the y launch
         r0 = c0 + w + t0 * 128
-        r1 = min(r0 + 128, N)
+        r1 = min(r0 + 128, ns)
         assert r0 < r1
         A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
+    elif kind == FWDLINV:
+        assert ns > PANEL and p == 0
+        X = dinv[("linv", s)]
+        r0 = t0 * PANEL
+        nr = min(PANEL, ns - r0)
+        assert nr > 0
+        B[first + r0:first + r0 + nr] = X[r0:r0 + nr, :r0 + nr] @ A[first:first + r0 + nr]
+    elif kind == BWDLINV:
+        assert ns > PANEL and p == 0
+        X = dinv[("linv", s)]
+        r0 = t0 * PANEL
+        nr = min(PANEL, ns - r0)
+        assert nr > 0
+        A[first + r0:first + r0 + nr] = X[r0:ns, r0:r0 + nr].T @ B[first + r0:first + ns]
     elif kind == BWDGEMM:
         xb = A[rows[ns:]]
         B[first + c0:first + c0 + w] -= F[ns:, c0:c0 + w].T @ xb

@@ -109,7 +109,7 @@ def test_schedule_counts_are_consistent():
     ops = nodal_operators(mesh, survey)
     sym = nat.Symbolic(ops.crow, ops.col, mesh.node_grid_index(), 64)
     for dtype in (0, 1):
-        for which in (0, 1, 2, 3):
+        for which in (0, 1, 2, 3, 4):
             tasks, launches = sym.schedule(dtype, which)
             assert launches[:, 3].sum() == tasks.shape[0]
             assert np.all(np.diff(launches[:, 2]) >= 0)
