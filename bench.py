@@ -48,6 +48,9 @@ WORKLOADS = {
                             "(x1.3), 96 electrodes, dipole-dipole + Wenner, nky 12"),
     "dc2d_small": dict(desc="2.5-D DC, TensorMesh 100x50 core @2.5 m + 10 padding "
                             "(x1.3), 21 electrodes, dipole-dipole n=1..6, nky 11"),
+    # a reduced 3-D case for profiler captures (a few GB on the device)
+    "dc3d_mid": dict(desc="3-D DC, TensorMesh 40x40x20 core @8 m + 6 padding/face "
+                          "(x1.3), same 200 sources and 6,000 data"),
 }
 # bounded CPU sample: the same workload family on a coarser grid
 CPU_SAMPLE = {
@@ -57,13 +60,16 @@ CPU_SAMPLE = {
                       "and 6,000 data; one full eval+grad per step"),
     "dc2d_large": dict(kw={}, desc="the full 2.5-D workload"),
     "dc2d_small": dict(kw={}, desc="the full 2.5-D workload"),
+    "dc3d_mid": dict(kw=dict(ncore=(24, 24, 12), dx=13.0, npad=4),
+                     desc="coarsened as for dc3d"),
 }
 
 
 def build_case(name, seed, sample=False):
     from simpeg_dc_torch_b200 import synthetic as syn
-    if name == "dc3d":
-        kw = CPU_SAMPLE["dc3d"]["kw"] if sample else {}
+    if name in ("dc3d", "dc3d_mid"):
+        kw = CPU_SAMPLE[name]["kw"] if sample else (
+            {} if name == "dc3d" else dict(ncore=(40, 40, 20), dx=8.0, npad=6))
         return syn.dc3d(seed=seed, **kw)
     if name == "dc2d_large":
         return syn.dc2d_large(seed=seed)
@@ -72,7 +78,7 @@ def build_case(name, seed, sample=False):
 
 def make_engine(name, mesh, survey, device, dtype):
     from simpeg_dc_torch_b200 import TorchDC2D, TorchDC3D
-    if name == "dc3d":
+    if name in ("dc3d", "dc3d_mid"):
         return TorchDC3D(mesh, survey, device=device, dtype=dtype)
     nky = 12 if name == "dc2d_large" else 11
     return TorchDC2D(mesh, survey, nky=nky, device=device, dtype=dtype)
@@ -147,7 +153,7 @@ def oracle_ops(name, mesh, survey):
     ops = nodal_operators(mesh, survey)
     op = dict(crow=ops.crow, col=ops.col, nN=ops.nN, Q=ops.q.toarray(),
               Pd=ops.Pd, sidx=ops.sidx)
-    if name == "dc3d":
+    if name.startswith("dc3d"):
         op["L3"] = ops.L3()
     else:
         nky = 12 if name == "dc2d_large" else 11
@@ -163,7 +169,7 @@ def cpu_eval_grad_timer(name, seed=0):
     from simpeg_dc_torch_b200 import synthetic as syn
     mesh, survey, m = build_case(name, seed, sample=True)
     op = oracle_ops(name, mesh, survey)
-    three_d = name == "dc3d"
+    three_d = name.startswith("dc3d")
     d = O.dpred_3d(op, m) if three_d else O.dpred_2d(op, m)
     dobs, w = syn.observed(d, np.random.default_rng(seed + 1))
 
@@ -209,19 +215,30 @@ def run_reference(args):
 
 # ------------------------------------------------------------------- ours
 def count_launches(eng):
-    """Kernels of libdct launched by one eval+grad (forward + adjoint)."""
+    """Kernels of libdct launched by one eval+grad (forward + adjoint),
+    counted from the plan's launch schedules (the same lists the library
+    walks) and the fixed launches of the fused path around them."""
     sym = eng.solver._sym
     code = eng.solver._code
-    per = {}
-    for which in (0, 1, 2):
+    nl = {}
+    for which in range(5):
         _, launches = sym.schedule(code, which)
-        per[which] = int((launches[:, 3] > 0).sum())
-    ir = 0 if code == 0 else eng.solver.refine
-    solve = (per[1] + per[2]) * (1 + ir) + (1 if code == 0 else 1 + (1 + ir) + ir)
-    # sigma + values, source scatter, projection, adjoint scatter, gather,
-    # values vjp; factor; two solves
-    # + the panel-inverse launch of the factorization
-    return per[0] + 1 + 2 * solve + 6
+        nl[which] = int((launches[:, 3] > 0).sum())
+    factor = nl[0] + nl[3] + nl[4] + (1 if code == 1 else 0)
+    passes = nl[1] + nl[2]
+    if code == 0:
+        solve = 1 + passes                       # rhs copy + substitution
+    else:
+        ir = eng.solver.refine
+        solve = 1 + (1 + ir) * (passes + 1) + ir  # + updates and residuals
+    # sigma/values (2), source scatter, projection, adjoint scatter,
+    # gather-contract, values vjp
+    return 7 + factor + 2 * solve
+
+
+# launch kinds whose dominant cost is tensor-core arithmetic (float32 plans)
+TENSOR_KINDS = {"trailing_update", "fwd_linv_tc", "fwd_bnd_tc", "bwd_gemm_tc",
+                "bwd_linv_tc"}
 
 
 def main():
@@ -291,7 +308,7 @@ def main():
            "grad_rel": float(torch.linalg.norm(g32 - g64) / torch.linalg.norm(g64)),
            "phi_rel": float(abs(phi32 - phi64) / abs(phi64))}
 
-    def timed(eng, steps, warmup, sampler=None):
+    def timed(eng, steps, warmup, sampler=None, tag=None):
         for _ in range(warmup):
             eval_grad(eng, m)
         torch.cuda.synchronize()
@@ -302,18 +319,22 @@ def main():
         st = torch.cuda.current_stream()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
+        if tag:   # NVTX range: lets a profiler select the timed launches
+            torch.cuda.nvtx.range_push(tag)
         a.record(st)
         for _ in range(steps):
             eval_grad(eng, m)
         b.record(st)
+        if tag:
+            torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         barrier()
         return max_over_ranks(a.elapsed_time(b) / steps), clocks
 
     sampler = ClockSampler(local)
-    ms32, clocks = timed(e32, args.steps, args.warmup, sampler)
-    ms64, _ = timed(e64, args.steps, args.warmup)
+    ms32, clocks = timed(e32, args.steps, args.warmup, sampler, tag="timed_fp32")
+    ms64, _ = timed(e64, args.steps, args.warmup, tag="timed_fp64")
 
     # end to end through the public API, host buffers in and out
     e2e = None
@@ -369,20 +390,30 @@ def main():
         peaks = _j.load(open(pk))
     hbm = peaks.get("hbm_gbs", 6650.0)
     tc = peaks.get("bf16_tflops", 1590.0)
-    compute_kinds = {"trailing_update", "small_front", "panel_trsm"}
-    if dom in compute_kinds:
+    traffic = None
+    tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tj):
+        traffic = _j.load(open(tj)).get(args.workload, {}).get(dom)
+    if dom in TENSOR_KINDS:
         ach = dfl / (dms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
-                "frac": ach / tc}
+                "frac": ach / tc,
+                "note": "3xTF32: three TF32 MMAs per product; the TF32 rate is "
+                        "half the bf16 rate, so this kernel's ceiling is "
+                        "peak/6 (frac_of_3xtf32_ceiling)",
+                "frac_of_3xtf32_ceiling": ach / (tc / 6.0)}
     else:
         ach = dby / (dms * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm}
     roof.update({"kernel": dom, "launches_per_step": dn / 2,
                  "avg_launch_ms": dms / max(dn, 1),
+                 "algorithmic_bytes_per_launch": dby / max(dn, 1),
+                 "algorithmic_flops_per_launch": dfl / max(dn, 1),
                  "share_of_solver_time": dms / tot if tot else None,
-                 "traffic": None,
-                 "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback"})
+                 "traffic": traffic,
+                 "peak_source": ("MEASURED_PEAKS.json (burst)" if peaks
+                                 else "fallback")})
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -82,7 +82,7 @@ int dct_symbolic_get_array(const dct_symbolic* sym, const char* name,
  * (which: 0 factorization, 1 forward, 2 backward substitution, 3 panel
  * inverses, 4 supernode inverses), for
  * inspection and CPU-side replay in tests.  tasks: 4 int32 per task
- * (supernode, panel, t0, t1); launches: 5 int64 per launch (kind, level,
+ * (supernode, panel or K start, t0, t1 or K end); launches: 5 int64 per launch (kind, level,
  * first task, task count, arg).  With null outputs only the counts are set. */
 int dct_symbolic_get_schedule(const dct_symbolic* sym, int32_t dtype,
                               int32_t which, int32_t* tasks, int64_t* ntasks,
@@ -127,12 +127,12 @@ int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
 /* Per-launch-kind timing with CUDA events on the launch stream (off by
  * default).  While enabled, every factor/solve launch is bracketed by events;
  * dct_plan_profile_get synchronises and returns, for one launch kind
- * (0 small fronts, 1 large scatter, 2 extend-add, 3 panel, 4 trailing
- * update, 5 forward step, 6 backward gemm, 7 backward step, 8 forward of
- * single-panel supernodes, 9 backward of single-panel supernodes, 10 panel
- * inverses, 11 forward row tiles on tensor cores, 12 forward boundary rows,
- * 13 forward boundary rows on tensor cores, 14-16 supernode-inverse steps,
- * 17 forward inverse products, 18 backward inverse products), the summed
+ * (0 small fronts, 1 large scatter, 2 extend-add, 3 panel TRSM, 4 trailing
+ * update, 5 panel inverses, 6-8 supernode-inverse steps, 9 forward of
+ * single-panel supernodes, 10 forward inverse products, 11 forward boundary
+ * rows, 12 backward of single-panel supernodes, 13 backward boundary
+ * product, 14 backward inverse products, 15-18 the products of 10, 11, 13
+ * and 14 on tensor cores in float32 plans), the summed
  * device milliseconds, the launch count and the algorithmic flops and bytes
  * of those launches; reset clears the counters. */
 int dct_plan_profile(dct_plan* plan, int32_t enable, int32_t reset);

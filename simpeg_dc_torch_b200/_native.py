@@ -225,10 +225,10 @@ class Plan:
                                        d_xp, stream), "dct_solve_permuted")
 
     KINDS = ("small_front", "large_scatter", "extend_add", "panel_trsm",
-             "trailing_update", "fwd_step", "bwd_gemm", "bwd_step",
-             "fwd_small", "bwd_small", "panel_inverse", "fwd_tc", "fwd_bnd",
-             "fwd_bnd_tc", "linv_init", "linv_t", "linv_x", "fwd_linv",
-             "bwd_linv")
+             "trailing_update", "panel_inverse", "linv_init", "linv_t",
+             "linv_x", "fwd_small", "fwd_linv", "fwd_bnd", "bwd_small",
+             "bwd_gemm", "bwd_linv", "fwd_linv_tc", "fwd_bnd_tc",
+             "bwd_gemm_tc", "bwd_linv_tc")
 
     def profile(self, enable, reset=True):
         check(lib().dct_plan_profile(self._h, int(bool(enable)), int(reset)),

@@ -131,6 +131,13 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
   }
 }
 
+// Tensor-core substitution tasks: one 128-row output tile t and a K range
+// [k0, k1) per task (PanelTask {s, k0, t, k1}); ranges longer than kTcSplitK
+// are split so that the top levels of the tree, which hold few supernodes,
+// still fill the GPU.  Within a launch the longest tasks come first.
+constexpr int kTcTile = 128;
+constexpr int kTcSplitK = 512;
+
 void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
   sc->flops.assign(sc->launches.size(), 0.0);
   sc->bytes.assign(sc->launches.size(), 0.0);
@@ -141,16 +148,11 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
     for (int64_t q = l.first; q < l.first + l.count; ++q) {
       const PanelTask& t = sc->tasks[q];
       const int s = t.s, N = S.front_n[s], ns = S.ns(s);
-      const int c0 = t.p * dct::kPanel, w = std::min(dct::kPanel, ns - c0);
       const double nbd = N - ns;
-      if (l.kind == dct::kFwdSmall) {
-        f += double(w) * w + 2 * nbd * w;
-        bf += es * (w * (w + 1) / 2.0 + nbd * w);
-        br += es * (2.0 * w + 2 * nbd);
-      } else if (l.kind == dct::kBwdSmall) {
-        f += double(w) * w + 2 * nbd * w;
-        bf += es * (w * (w + 1) / 2.0 + nbd * w);
-        br += es * (2.0 * w + nbd);
+      if (l.kind == dct::kFwdSmall || l.kind == dct::kBwdSmall) {
+        f += double(ns) * ns + 2 * nbd * ns;
+        bf += es * (ns * (ns + 1) / 2.0 + nbd * ns);
+        br += es * (2.0 * ns + (l.kind == dct::kFwdSmall ? 2 : 1) * nbd);
       } else if (l.kind == dct::kFwdLinv || l.kind == dct::kBwdLinv) {
         const double nr = std::min(dct::kPanel, ns - t.t0 * dct::kPanel);
         const double kk = l.kind == dct::kFwdLinv ? (t.t0 * dct::kPanel + nr)
@@ -158,43 +160,32 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
         f += 2 * nr * kk;
         bf += es * nr * kk;
         br += es * (nr + kk);
-      } else if (l.kind == dct::kFwdBnd || l.kind == dct::kFwdBndTc) {
-        const int tile = l.kind == dct::kFwdBndTc ? 128 : dct::kPanel;
-        const double nr = std::min(tile, N - (ns + t.t0 * tile));
+      } else if (l.kind == dct::kFwdBnd) {
+        const double nr = std::min(dct::kPanel, N - (ns + t.t0 * dct::kPanel));
         f += 2 * nr * ns;
         bf += es * nr * ns;
         br += es * (2 * nr + ns);
-      } else if (l.kind == dct::kFwdTc) {
-        const int r0 = c0 + w + t.t0 * 128;
-        const double nr = std::min(128, N - r0);
-        f += 2 * nr * w;
-        bf += es * nr * w;
-        br += es * (2 * nr + w);
-      } else if (l.kind == dct::kFwdStep) {
-        if (t.t0 == 0) {
-          f += double(w) * w;
-          bf += es * w * (w + 1) / 2.0;
-          br += es * 2.0 * w;
-        } else {
-          const int r0 = c0 + w + (t.t0 - 1) * dct::kPanel;
-          const double nr = std::min(t.t1 * dct::kPanel + c0 + w, N) - r0;
-          f += 2 * nr * w;
-          bf += es * nr * w;
-          br += es * 2 * nr;
-        }
       } else if (l.kind == dct::kBwdGemm) {
+        const double w = std::min(dct::kPanel, ns - t.p * dct::kPanel);
         f += 2 * nbd * w;
         bf += es * nbd * w;
         br += es * (nbd + 2.0 * w);
-      } else if (l.kind == dct::kBwdStep) {
-        f += double(w) * w;
-        bf += es * w * (w + 1) / 2.0;
-        br += es * 2.0 * w;
-        if (t.t0 != t.p) {
-          f += 2.0 * w * dct::kPanel;
-          bf += es * w * dct::kPanel;
-          br += es * 2.0 * dct::kPanel;
+      } else if (l.kind >= dct::kFwdLinvTc && l.kind <= dct::kBwdLinvTc) {
+        // entries of the A tile that are used (the inverses are triangular)
+        const int m0 = t.t0 * kTcTile;
+        const int mr = std::min(kTcTile, (l.kind == dct::kFwdBndTc ? N - ns : ns) - m0);
+        double used = 0;
+        if (l.kind == dct::kFwdLinvTc || l.kind == dct::kBwdLinvTc) {
+          for (int m = m0; m < m0 + mr; ++m)
+            used += l.kind == dct::kFwdLinvTc
+                        ? std::max(0, std::min(t.t1, m + 1) - t.p)
+                        : std::max(0, t.t1 - std::max(t.p, m));
+        } else {
+          used = double(mr) * (t.t1 - t.p);
         }
+        f += 2 * used;
+        bf += es * used;
+        br += es * ((t.t1 - t.p) + 2.0 * mr);
       }
     }
     sc->flops[li] = f;
@@ -288,14 +279,23 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile,
 // (kFwdLinv / kBwdLinv, 64-row tiles) and exchange with their boundary rows
 // once (kFwdBnd[Tc] after, kBwdGemm before).  A pass is a few launches per
 // level, independent of the supernodes' widths.
+void push_split(std::vector<PanelTask>& T, int s, int t, int k0, int k1) {
+  for (int a = k0; a < k1; a += kTcSplitK) T.push_back({s, a, t, std::min(k1, a + kTcSplitK)});
+}
+
 void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
                            dct::Schedule* bwd) {
   const bool tc = dtype == DCT_F32;
   auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel; };
-  auto add = [](dct::Schedule* sc, int kind, int lv, auto&& fill) {
+  auto add = [&](dct::Schedule* sc, int kind, int lv, auto&& fill) {
     Launch l{kind, lv, int64_t(sc->tasks.size()), 0, 0};
     fill(sc->tasks);
     l.count = int64_t(sc->tasks.size()) - l.first;
+    if (tc && l.count)
+      std::stable_sort(sc->tasks.begin() + l.first, sc->tasks.end(),
+                       [](const PanelTask& x, const PanelTask& y) {
+                         return x.t1 - x.p > y.t1 - y.p;
+                       });
     if (l.count) sc->launches.push_back(l);
   };
   for (int lv = 0; lv < S.nlevels; ++lv) {
@@ -304,19 +304,27 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
       for (int q = q0; q < q1; ++q)
         if (is_small(S.level_sn[q])) T.push_back({S.level_sn[q], 0, 0, 0});
     });
-    add(fwd, dct::kFwdLinv, lv, [&](std::vector<PanelTask>& T) {
+    add(fwd, tc ? dct::kFwdLinvTc : dct::kFwdLinv, lv, [&](std::vector<PanelTask>& T) {
       for (int q = q0; q < q1; ++q) {
-        const int s = S.level_sn[q];
+        const int s = S.level_sn[q], ns = S.ns(s);
         if (is_small(s)) continue;
-        for (int t = 0; t * dct::kPanel < S.ns(s); ++t) T.push_back({s, 0, t, 0});
+        if (tc) {
+          for (int t = 0; t * kTcTile < ns; ++t)
+            push_split(T, s, t, 0, std::min(ns, (t + 1) * kTcTile));
+        } else {
+          for (int t = 0; t * dct::kPanel < ns; ++t) T.push_back({s, 0, t, 0});
+        }
       }
     });
-    const int tile = tc ? 128 : dct::kPanel;
     add(fwd, tc ? dct::kFwdBndTc : dct::kFwdBnd, lv, [&](std::vector<PanelTask>& T) {
       for (int q = q0; q < q1; ++q) {
         const int s = S.level_sn[q];
         if (is_small(s)) continue;
-        for (int t = 0; t < ceil_div(S.nb(s), tile); ++t) T.push_back({s, 0, t, 0});
+        if (tc) {
+          for (int t = 0; t < ceil_div(S.nb(s), kTcTile); ++t) push_split(T, s, t, 0, S.ns(s));
+        } else {
+          for (int t = 0; t < ceil_div(S.nb(s), dct::kPanel); ++t) T.push_back({s, 0, t, 0});
+        }
       }
     });
   }
@@ -326,18 +334,26 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
       for (int q = q0; q < q1; ++q)
         if (is_small(S.level_sn[q])) T.push_back({S.level_sn[q], 0, 0, 0});
     });
-    add(bwd, dct::kBwdGemm, lv, [&](std::vector<PanelTask>& T) {
+    add(bwd, tc ? dct::kBwdGemmTc : dct::kBwdGemm, lv, [&](std::vector<PanelTask>& T) {
       for (int q = q0; q < q1; ++q) {
-        const int s = S.level_sn[q];
+        const int s = S.level_sn[q], ns = S.ns(s);
         if (is_small(s) || S.nb(s) == 0) continue;
-        for (int p = 0; p * dct::kPanel < S.ns(s); ++p) T.push_back({s, p, 0, 0});
+        if (tc) {
+          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, 0, S.nb(s));
+        } else {
+          for (int p = 0; p * dct::kPanel < ns; ++p) T.push_back({s, p, 0, 0});
+        }
       }
     });
-    add(bwd, dct::kBwdLinv, lv, [&](std::vector<PanelTask>& T) {
+    add(bwd, tc ? dct::kBwdLinvTc : dct::kBwdLinv, lv, [&](std::vector<PanelTask>& T) {
       for (int q = q0; q < q1; ++q) {
-        const int s = S.level_sn[q];
+        const int s = S.level_sn[q], ns = S.ns(s);
         if (is_small(s)) continue;
-        for (int t = 0; t * dct::kPanel < S.ns(s); ++t) T.push_back({s, 0, t, 0});
+        if (tc) {
+          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, t * kTcTile, ns);
+        } else {
+          for (int t = 0; t * dct::kPanel < ns; ++t) T.push_back({s, 0, t, 0});
+        }
       }
     });
   }

@@ -43,22 +43,22 @@ enum LaunchKind : int {
   kSmallFront = 0,   // fused assemble + partial Cholesky, one CTA per front
   kLargeScatter,     // matrix entries into large fronts
   kLargeExtendAdd,   // one child slot into large fronts
-  kLargePanel,       // diagonal block Cholesky + TRSM of the rows below
-  kLargeUpdate,      // trailing symmetric update tiles
-  kFwdStep,          // forward substitution, one panel step
-  kBwdGemm,          // backward: subtract boundary-row contributions
-  kBwdStep,          // backward substitution, one panel step
-  kFwdSmall,         // forward substitution of single-panel supernodes
-  kBwdSmall,         // backward substitution of single-panel supernodes
-  kPanelInverse,     // inverses of the factored diagonal blocks
-  kFwdTc,            // forward row-tile updates on tensor cores (float32)
-  kFwdBnd,           // forward boundary-row update of a supernode (float64)
-  kFwdBndTc,         // the same on tensor cores (float32)
+  kLargePanel,       // TRSM of the rows below a factored diagonal block
+  kLargeUpdate,      // trailing symmetric update tiles (+ next diagonal block)
+  kPanelInverse,     // inverses of the diagonal blocks of single-CTA fronts
   kLinvInit,         // supernode inverses: diagonal 64-blocks from the panels
   kLinvT,            // supernode inverses, doubling step T = C A^{-1}
   kLinvX,            // supernode inverses, doubling step X = -D^{-1} T
-  kFwdLinv,          // forward: y_s = L_ss^{-1} b_s for large supernodes
-  kBwdLinv,          // backward: x_s = L_ss^{-T} y_s for large supernodes
+  kFwdSmall,         // forward substitution of single-panel supernodes
+  kFwdLinv,          // forward: y_s = L_ss^{-1} b_s, large supernodes (f64)
+  kFwdBnd,           // forward: boundary rows -= L_Bs y_s (f64)
+  kBwdSmall,         // backward substitution of single-panel supernodes
+  kBwdGemm,          // backward: y_s -= L_Bs^T x_B (f64)
+  kBwdLinv,          // backward: x_s = L_ss^{-T} y_s (f64)
+  kFwdLinvTc,        // the four products above on tensor cores (f32),
+  kFwdBndTc,         //   128-row output tiles, split K ranges
+  kBwdGemmTc,
+  kBwdLinvTc,
   kNumKinds
 };
 
@@ -143,6 +143,29 @@ struct dct_symbolic {
 };
 
 namespace dct {
+// arguments of the substitution kernels (solve.cu, solve_tc.cu)
+template <typename T>
+struct SolveArgs {
+  DevSym S;
+  const PanelTask* tasks;
+  const T* fronts;
+  int64_t front_stride;
+  const T* dinv;
+  const int64_t* dinv_off;
+  int64_t dinv_stride;
+  T* A;
+  T* B;
+  int n, k, nchunk;
+  int* status;
+  const T* linv;
+  const int64_t* linv_off;
+  int64_t linv_stride;
+};
+// right-hand sides per CTA of the tensor-core substitution kernels
+constexpr int kSolveTcRhs = 256;
+// one launch of a tensor-core substitution kind (kFwdLinvTc .. kBwdLinvTc)
+cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g, int64_t count,
+                            int nbatch, cudaStream_t st);
 // records the message returned by dct_last_error() for this thread
 void set_last_error(const char* msg);
 cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,

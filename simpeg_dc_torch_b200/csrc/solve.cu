@@ -1,28 +1,30 @@
 // Multi-RHS supernodal substitution L L^T x = b for nbatch systems, in the
 // permuted order, on row-major (n, k) right-hand sides.
 //
-// The inverse of every 64-column panel's diagonal block, D_p^{-1}, is formed
-// once after the factorization (k_panel_inverse), so each panel solve is a
-// small matrix product instead of a serial triangular sweep.
+// Per tree level (forward bottom-up, backward top-down):
+//   supernodes of one panel (ns <= 64): one CTA per (supernode, system, 64
+//     right-hand sides) does the whole step with the stored panel inverse
+//     D^{-1} (k_fwd_small / k_bwd_small);
+//   larger supernodes: products with the explicit supernode inverse
+//     L_ss^{-1} (formed after the factorization) and with the boundary block
+//     L_Bs, in 64-row tiles on CUDA cores (float64 plans: k_fwd_linv,
+//     k_fwd_bnd, k_bwd_gemm, k_bwd_linv) or in 128-row tiles on the tensor
+//     cores (float32 plans, solve_tc.cu).
 //
 // Two work buffers A and B of nbatch*n*k elements are used so that no launch
 // ever reads a location that another CTA of the same launch writes:
-//   forward  (levels bottom-up): the right-hand side b lives in A and receives
-//            the updates -L_below y_p (plain stores for rows of the same
-//            supernode, atomics for its boundary rows, which other supernodes
-//            of the level may also update); y_p = D_p^{-1} b_p goes to B.
-//   backward (levels top-down): y_p -= L_{B,p}^T x_B (x_B: final rows of
-//            ancestors, in A); x_p = D_p^{-T} y_p goes to A and
-//            y_i -= L_{p,i}^T x_p updates the earlier panels in B.
-// Supernodes of one panel are handled by one CTA per (supernode, system,
-// 64 right-hand sides) in each direction.  Larger supernodes run panel steps
-// whose CTAs recompute the panel's small product instead of waiting for
-// another CTA: no inter-CTA synchronisation exists anywhere.
+//   forward:  b lives in A and receives the updates -L_Bs y_s of the rows
+//             below (atomics: several supernodes of a level may share
+//             ancestor rows); y_s goes to B.
+//   backward: y_s -= L_Bs^T x_B with x_B (rows of ancestors, final) in A;
+//             x_s = L_ss^{-T} y_s goes to A.
+// The tensor-core kinds split long K ranges over CTAs and accumulate with
+// atomics, so in float32 plans B is cleared before the forward pass and A
+// (whose right-hand side is consumed by then) before the backward pass.
 #include <cuda_runtime.h>
 
 #include "dct_internal.h"
 #include "tile_mm.cuh"
-#include "tc_common.cuh"
 
 namespace dct {
 namespace {
@@ -75,24 +77,6 @@ __device__ __forceinline__ void load_dinv(T* S, const T* __restrict__ Di, int w,
     else S[c * kLD1 + r] = v;
   }
 }
-
-template <typename T>
-struct SolveArgs {
-  DevSym S;
-  const PanelTask* tasks;
-  const T* fronts;
-  int64_t front_stride;
-  const T* dinv;
-  const int64_t* dinv_off;
-  int64_t dinv_stride;
-  T* A;
-  T* B;
-  int n, k, nchunk;
-  int* status;
-  const T* linv;
-  const int64_t* linv_off;
-  int64_t linv_stride;
-};
 
 // ------------------------------------------------------------ forward, small
 // one CTA: y = D^{-1} b (to B), then b[boundary rows] -= L_B y (atomics, A)
@@ -152,207 +136,6 @@ __global__ void __launch_bounds__(kThreads) k_fwd_small(SolveArgs<T> g) {
   }
 }
 
-// ------------------------------------------------------------ forward, step
-// large supernodes, panel p.  t0 = 0: y_p = D_p^{-1} b_p to B.  t0 >= 1: row
-// tiles [t0-1, t1) below the panel (64 rows each) receive -L y_p in A.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd_step(SolveArgs<T> g) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* S1 = reinterpret_cast<T*>(smem_raw);
-  T* S2 = S1 + kLD1 * kLD;
-  T* Y = S2 + kLD * kLD;
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
-  const int rc = min(kRC, g.k - j0);
-  const DevSym& S = g.S;
-  const int s = tk.s;
-  const int N = S.front_n[s], first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
-  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
-  T* A = g.A + int64_t(b) * g.n * g.k;
-  T* Bo = g.B + int64_t(b) * g.n * g.k;
-  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
-  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s] + int64_t(tk.p) * kPanel * kPanel,
-            w, false);
-  load_rhs(S2, A, g.k, j0, rc, w, nullptr, first + c0);
-  __syncthreads();
-  T acc[4][4];
-  zero_acc(acc);
-  mm_tile(S1, S2, w, w, acc);
-  if (tk.t0 == 0) {
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = ag + 16 * p, j = jg + 16 * q;
-        if (r < w && j < rc) Bo[int64_t(first + c0 + r) * g.k + j0 + j] = acc[p][q];
-      }
-    return;
-  }
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) Y[(ag + 16 * p) * kLD + jg + 16 * q] = acc[p][q];
-  const int32_t* rows = S.rows + S.rows_ptr[s];
-  for (int t = tk.t0 - 1; t < tk.t1; ++t) {
-    const int r0 = c0 + w + t * kLD;
-    const int nr = min(kLD, ns - r0);   // own rows only; boundary rows: k_fwd_bnd
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
-      const int r = idx % kLD, c = idx / kLD;
-      S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c0 + c) * N] : T(0);
-    }
-    __syncthreads();
-    zero_acc(acc);
-    mm_tile(S1, Y, w, nr, acc);
-    T cur[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const int r = ag + 16 * p;
-      const bool own = r < nr && r0 + r < ns;
-      const T* src = own ? A + int64_t(rows[r0 + r]) * g.k + j0 : nullptr;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j = jg + 16 * q;
-        cur[p][q] = (own && j < rc) ? src[j] : T(0);
-      }
-    }
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const int r = ag + 16 * p;
-      if (r >= nr) continue;
-      const int lr = r0 + r;
-      T* dst = A + int64_t(rows[lr]) * g.k + j0;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j = jg + 16 * q;
-        if (j >= rc) continue;
-        if (lr < ns) dst[j] = cur[p][q] - acc[p][q];
-        else atomic_sub(dst + j, acc[p][q]);
-      }
-    }
-  }
-}
-
-// ------------------------------------------------------------ forward, tensor cores
-// float32 plans, large supernodes, panel p: one 128-row tile t0 below the
-// panel receives -L_tile y_p for up to 256 right-hand sides at once
-// (tcgen05.mma kind::tf32, 3xTF32, M = 128, N = right-hand sides rounded up
-// to 16).  y_p was written to B by the preceding launch (k_fwd_step, t0 = 0).
-constexpr int kTcRhs = 256;                              // N per CTA
-constexpr int kTcRhsBytes = kTcRhs * 64 * 4;             // one B operand
-constexpr size_t kFwdTcSmem = 2 * size_t(kTcOperandBytes) + 2 * size_t(kTcRhsBytes) + 64;
-
-__global__ void __launch_bounds__(kTcThreads, 1) k_fwd_tc(SolveArgs<float> g) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* Ahi = smem_raw;
-  unsigned char* Alo = Ahi + kTcOperandBytes;
-  unsigned char* Bhi = Alo + kTcOperandBytes;
-  unsigned char* Blo = Bhi + kTcRhsBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcRhsBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kTcRhs;
-  const int kc = min(kTcRhs, g.k - j0);
-  const int np = (kc + 15) & ~15;
-  const DevSym& S = g.S;
-  const int s = tk.s;
-  const int N = S.front_n[s], first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
-  const int r0 = c0 + w + tk.t0 * kTcM;
-  const int nr = min(kTcM, ns - r0);   // own rows only; boundary rows: k_fwd_bnd_tc
-  const float* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
-  float* A = g.A + int64_t(b) * g.n * g.k;
-  const float* Bo = g.B + int64_t(b) * g.n * g.k;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-  if (warp == 0) tmem_alloc(tmem_slot, kTcRhs);
-  if (tid == 0) mbar_init(mbar);
-  // A: the L rows of the tile (m = tile row, k = panel column); all of a
-  // warp's loads are issued before its shared stores
-  {
-    constexpr int kWarps = kTcThreads / 32, kPer = (kTcM / 8) * 16 / kWarps;
-    const int m_lo = lane >> 2, k_lo = lane & 3;
-    float v[kPer];
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int cm = warp + u * kWarps;
-      const int m = (cm % (kTcM / 8)) * 8 + m_lo, kq = (cm / (kTcM / 8)) * 4 + k_lo;
-      v[u] = (m < nr && kq < w) ? F[(r0 + m) + int64_t(c0 + kq) * N] : 0.0f;
-    }
-#pragma unroll
-    for (int u = 0; u < kPer; ++u) {
-      const int cm = warp + u * kWarps;
-      tc_store_split(Ahi, Alo,
-                     (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
-                     v[u]);
-    }
-  }
-  // B: y_p^T (n = right-hand side, k = panel row), read row-wise from B
-  {
-    constexpr int kWarps = kTcThreads / 32;
-    const int ncm = (np / 8) * 16;
-    const int j_lo = lane >> 2, k_lo = lane & 3;
-    for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
-      float v[16];
-#pragma unroll
-      for (int u = 0; u < 16; ++u) {
-        const int cm = c0m + warp + u * kWarps;
-        const int j = (cm % (np / 8)) * 8 + j_lo, kq = (cm / (np / 8)) * 4 + k_lo;
-        v[u] = (cm < ncm && j < kc && kq < w)
-                   ? Bo[int64_t(first + c0 + kq) * g.k + j0 + j] : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < 16; ++u) {
-        const int cm = c0m + warp + u * kWarps;
-        if (cm < ncm)
-          tc_store_split(Bhi, Blo,
-                         (cm % (np / 8)) * kTcSBO + (cm / (np / 8)) * kTcLBO + lane * 4,
-                         v[u]);
-      }
-    }
-  }
-  tc_publish_smem();
-  const uint32_t tmem = *tmem_slot;
-  if (tid == 0)
-    umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
-                (w + 7) / 8, umma_idesc_tf32(kTcM, np), 0, mbar);
-  const bool done = tc_wait(mbar, 0, g.status,
-                            DCT_ERR_DEVICE_TIMEOUT, s, b);
-  if (done) {
-    const int row = (warp & 3) * 32 + lane;
-    const int32_t* rows = S.rows + S.rows_ptr[s];
-    const int lr = r0 + row;
-    const bool own = lr < ns;            // a pivot row of this supernode
-    float* dst = (row < nr) ? A + int64_t(rows[lr]) * g.k + j0 : nullptr;
-    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
-      uint32_t v[32];
-      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
-      if (dst != nullptr) {
-        if (own) {
-          float cur[32];
-#pragma unroll
-          for (int c = 0; c < 32; ++c) cur[c] = (cb + c < kc) ? dst[cb + c] : 0.0f;
-#pragma unroll
-          for (int c = 0; c < 32; ++c)
-            if (cb + c < kc) dst[cb + c] = cur[c] - __uint_as_float(v[c]);
-        } else {
-#pragma unroll
-          for (int c = 0; c < 32; ++c)
-            if (cb + c < kc) atomicAdd(dst + cb + c, -__uint_as_float(v[c]));
-        }
-      }
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, kTcRhs);
-}
-
 // ------------------------------------------------------------ forward, boundary
 // large supernodes, after all of their panel steps: the 64-row tile t of the
 // boundary rows [ns, N) receives -L[tile, 0:ns] y_s (y_s = all panels, in B),
@@ -401,109 +184,6 @@ __global__ void __launch_bounds__(kThreads) k_fwd_bnd(SolveArgs<T> g) {
       if (j < rc) atomic_sub(dst + j, acc[p][q]);
     }
   }
-}
-
-// float32: the same boundary update on the tensor cores, 128 rows per CTA,
-// all right-hand sides (<= 256) per MMA, K = ns in steps of one panel with
-// the accumulator kept in TMEM.
-__global__ void __launch_bounds__(kTcThreads, 1) k_fwd_bnd_tc(SolveArgs<float> g) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* Ahi = smem_raw;
-  unsigned char* Alo = Ahi + kTcOperandBytes;
-  unsigned char* Bhi = Alo + kTcOperandBytes;
-  unsigned char* Blo = Bhi + kTcRhsBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcRhsBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kTcRhs;
-  const int kc = min(kTcRhs, g.k - j0);
-  const int np = (kc + 15) & ~15;
-  const DevSym& S = g.S;
-  const int s = tk.s;
-  const int N = S.front_n[s], first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int r0 = ns + tk.t0 * kTcM;
-  const int nr = min(kTcM, N - r0);
-  const float* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
-  float* A = g.A + int64_t(b) * g.n * g.k;
-  const float* Bo = g.B + int64_t(b) * g.n * g.k;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int kWarps = kTcThreads / 32;
-  if (warp == 0) tmem_alloc(tmem_slot, kTcRhs);
-  if (tid == 0) mbar_init(mbar);
-  __syncthreads();
-  const uint32_t idesc = umma_idesc_tf32(kTcM, np);
-  bool ok = true;
-  int phase = 0;
-  for (int c0 = 0; c0 < ns && ok; c0 += kPanel, ++phase) {
-    const int w = min(kPanel, ns - c0);
-    {
-      constexpr int kPer = (kTcM / 8) * 16 / kWarps;
-      const int m_lo = lane >> 2, k_lo = lane & 3;
-      float v[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int cm = warp + u * kWarps;
-        const int m = (cm % (kTcM / 8)) * 8 + m_lo, kq = (cm / (kTcM / 8)) * 4 + k_lo;
-        v[u] = (m < nr && kq < w) ? F[(r0 + m) + int64_t(c0 + kq) * N] : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int cm = warp + u * kWarps;
-        tc_store_split(Ahi, Alo,
-                       (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
-                       v[u]);
-      }
-    }
-    {
-      const int ncm = (np / 8) * 16;
-      const int j_lo = lane >> 2, k_lo = lane & 3;
-      for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
-        float v[16];
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int cm = c0m + warp + u * kWarps;
-          const int j = (cm % (np / 8)) * 8 + j_lo, kq = (cm / (np / 8)) * 4 + k_lo;
-          v[u] = (cm < ncm && j < kc && kq < w)
-                     ? Bo[int64_t(first + c0 + kq) * g.k + j0 + j] : 0.0f;
-        }
-#pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int cm = c0m + warp + u * kWarps;
-          if (cm < ncm)
-            tc_store_split(Bhi, Blo,
-                           (cm % (np / 8)) * kTcSBO + (cm / (np / 8)) * kTcLBO + lane * 4,
-                           v[u]);
-        }
-      }
-    }
-    tc_publish_smem();
-    const uint32_t tmem = *tmem_slot;
-    if (tid == 0)
-      umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
-                  (w + 7) / 8, idesc, c0 > 0 ? 1u : 0u, mbar);
-    // the operands may be overwritten only after these MMAs completed
-    ok = tc_wait(mbar, uint32_t(phase & 1), g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
-  }
-  const uint32_t tmem = *tmem_slot;
-  if (ok) {
-    const int row = (warp & 3) * 32 + lane;
-    const int32_t* rows = S.rows + S.rows_ptr[s];
-    float* dst = (row < nr) ? A + int64_t(rows[r0 + row]) * g.k + j0 : nullptr;
-    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
-      uint32_t v[32];
-      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
-      if (dst != nullptr) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-          if (cb + c < kc) atomicAdd(dst + cb + c, -__uint_as_float(v[c]));
-      }
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, kTcRhs);
 }
 
 // ------------------------------------------------------------ inverse products
@@ -693,75 +373,6 @@ __global__ void __launch_bounds__(kThreads) k_bwd_gemm(SolveArgs<T> g) {
     }
 }
 
-// ------------------------------------------------------------ backward step
-// large supernodes, panel p: x_p = D_p^{-T} y_p.  t0 == p: write x_p to A;
-// t0 = i < p: y_i (B) -= L[panel p rows, panel i cols]^T x_p.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_bwd_step(SolveArgs<T> g) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* S1 = reinterpret_cast<T*>(smem_raw);
-  T* S2 = S1 + kLD1 * kLD;
-  T* X = S2 + kLD * kLD;
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
-  const int rc = min(kRC, g.k - j0);
-  const DevSym& S = g.S;
-  const int s = tk.s;
-  const int N = S.front_n[s], first = S.sn_first[s];
-  const int ns = S.sn_first[s + 1] - first;
-  const int c0 = tk.p * kPanel, w = min(kPanel, ns - c0);
-  const T* F = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
-  T* A = g.A + int64_t(b) * g.n * g.k;
-  T* Bo = g.B + int64_t(b) * g.n * g.k;
-  const int jg = threadIdx.x & 15, ag = threadIdx.x >> 4;
-  load_dinv(S1, g.dinv + b * g.dinv_stride + g.dinv_off[s] + int64_t(tk.p) * kPanel * kPanel,
-            w, true);
-  load_rhs(S2, Bo, g.k, j0, rc, w, nullptr, first + c0);
-  __syncthreads();
-  T acc[4][4];
-  zero_acc(acc);
-  mm_tile(S1, S2, w, w, acc);
-  if (tk.t0 == tk.p) {
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int r = ag + 16 * p, j = jg + 16 * q;
-        if (r < w && j < rc) A[int64_t(first + c0 + r) * g.k + j0 + j] = acc[p][q];
-      }
-    return;
-  }
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) X[(ag + 16 * p) * kLD + jg + 16 * q] = acc[p][q];
-  const int ci0 = tk.t0 * kPanel;     // earlier panels are full width
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
-    const int r = idx % kLD, c = idx / kLD;
-    S1[r * kLD1 + c] = (r < w) ? F[(c0 + r) + int64_t(ci0 + c) * N] : T(0);
-  }
-  __syncthreads();
-  zero_acc(acc);
-  mm_tile(S1, X, w, kLD, acc);
-  T cur[4][4];
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int c = ag + 16 * p, j = jg + 16 * q;
-      cur[p][q] = (j < rc) ? Bo[int64_t(first + ci0 + c) * g.k + j0 + j] : T(0);
-    }
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int c = ag + 16 * p, j = jg + 16 * q;
-      if (j < rc) Bo[int64_t(first + ci0 + c) * g.k + j0 + j] = cur[p][q] - acc[p][q];
-    }
-}
-
 // ------------------------------------------------------------ permutations
 template <typename TI, typename TO>
 __global__ void k_perm_in(const TI* __restrict__ b, int64_t bstride,
@@ -861,10 +472,8 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
                            reinterpret_cast<const void*>(k_fwd_bnd<T>),
                            reinterpret_cast<const void*>(k_fwd_linv<T>),
                            reinterpret_cast<const void*>(k_bwd_linv<T>),
-                           reinterpret_cast<const void*>(k_fwd_step<T>),
                            reinterpret_cast<const void*>(k_bwd_small<T>),
-                           reinterpret_cast<const void*>(k_bwd_gemm<T>),
-                           reinterpret_cast<const void*>(k_bwd_step<T>)};
+                           reinterpret_cast<const void*>(k_bwd_gemm<T>)};
   for (const void* kf : kernels) {
     e = cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem3));
@@ -874,16 +483,15 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
                  static_cast<const T*>(P->dinv), P->d_dinv_off, P->dinv_stride,
                  bufA, bufB, P->sym.n, k, nchunk, P->status,
                  static_cast<const T*>(P->linv), P->d_linv_off, P->linv_stride};
-  if constexpr (sizeof(T) == 4) {
-    e = cudaFuncSetAttribute(k_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kFwdTcSmem));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(k_fwd_bnd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kFwdTcSmem));
-    if (e != cudaSuccess) return e;
-  }
+  constexpr bool kTc = sizeof(T) == 4;
+  const size_t work = sizeof(T) * size_t(P->nbatch) * P->sym.n * k;
   const double nb = P->nbatch;
   for (const Schedule* sc : {&P->fwd, &P->bwd}) {
+    if (kTc) {
+      e = cudaMemsetAsync(sc == &P->fwd ? static_cast<void*>(bufB) : static_cast<void*>(bufA),
+                          0, work, st);
+      if (e != cudaSuccess) return e;
+    }
     for (size_t li = 0; li < sc->launches.size(); ++li) {
       const Launch& L = sc->launches[li];
       if (L.count <= 0) continue;
@@ -893,29 +501,23 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
         return e;
       g.tasks = sc->d_tasks + L.first;
       dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
-      if (L.kind == kFwdTc || L.kind == kFwdBndTc) {
-        if constexpr (sizeof(T) == 4) {
-          SolveArgs<float> gt = g;
-          gt.nchunk = (k + kTcRhs - 1) / kTcRhs;
-          dim3 gg(static_cast<unsigned>(L.count), P->nbatch * gt.nchunk);
-          if (L.kind == kFwdTc) k_fwd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
-          else k_fwd_bnd_tc<<<gg, kTcThreads, kFwdTcSmem, st>>>(gt);
-        } else {
-          return cudaErrorInvalidValue;
-        }
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if ((e = P->prof.end(st)) != cudaSuccess) return e;
-        continue;
-      }
       switch (L.kind) {
         case kFwdSmall: k_fwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
-        case kFwdStep: k_fwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kFwdBnd: k_fwd_bnd<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kFwdLinv: k_fwd_linv<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdLinv: k_bwd_linv<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdSmall: k_bwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kBwdGemm: k_bwd_gemm<T><<<grid, kThreads, smem3, st>>>(g); break;
-        case kBwdStep: k_bwd_step<T><<<grid, kThreads, smem3, st>>>(g); break;
+        case kFwdLinvTc:
+        case kFwdBndTc:
+        case kBwdGemmTc:
+        case kBwdLinvTc:
+          if constexpr (kTc) {
+            e = launch_solve_tc(L.kind, g, L.count, P->nbatch, st);
+            if (e != cudaSuccess) return e;
+            break;
+          }
+          return cudaErrorInvalidValue;
         default: return cudaErrorInvalidValue;
       }
       if ((e = cudaGetLastError()) != cudaSuccess) return e;

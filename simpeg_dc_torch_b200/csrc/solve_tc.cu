@@ -1,0 +1,249 @@
+// Float32 substitution products of the large supernodes on the tensor cores.
+//
+// Each of the four block products of the supernodal substitution is one
+// launch kind of the same kernel, D (128 x N) = sum_k A[m, k] B[k, n], with
+// the N right-hand sides (<= 256 per CTA) as the MMA's N dimension:
+//
+//   kFwdLinvTc  y_s   += L_ss^{-1}[rows m, k] b_s[k]        (B <- A rows)
+//   kFwdBndTc   b_B   -= L_Bs[rows m, k] y_s[k]             (A rows, gathered)
+//   kBwdGemmTc  y_s   -= L_Bs^T[cols m, k] x_B[k]           (B <- gathered A)
+//   kBwdLinvTc  x_s   += L_ss^{-T}[cols m, k] y_s[k]        (A <- B rows)
+//
+// A task covers one 128-row tile of the output and a K range [k0, k1); a
+// product whose K range is split over several tasks accumulates with float
+// atomics, so the destination rows of the two inverse products are cleared
+// before the pass that writes them (see solve.cu).  tcgen05.mma kind::tf32
+// with the 3xTF32 split (hi*hi + hi*lo + lo*hi: Markidis et al. 2018; Ootomo
+// and Yokota 2022) accumulates in TMEM; operands are staged through registers
+// (the split needs them there) into a two-stage shared-memory ring so that
+// the loads of stage i+1 overlap the MMAs of stage i.
+#include <cuda_runtime.h>
+
+#include "dct_internal.h"
+#include "tc_common.cuh"
+
+namespace dct {
+namespace {
+
+constexpr int kStK = 32;                     // K per pipeline stage
+constexpr int kStN = 256;                    // right-hand sides per CTA
+constexpr int kWarps = kTcThreads / 32;
+// A operand (128 x 32): K-adjacent core matrices 160 B apart, so that the
+// transposed loaders (2 rows x 16 K per warp instruction) and the natural
+// ones (8 rows x 4 K) both store to 32 distinct banks.
+constexpr uint32_t kALbo = 160, kASbo = 7 * kALbo + 128;      // 1248
+constexpr int kABytes = (kTcM / 8) * kASbo;                    // 19968
+constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo;   // 1024
+constexpr int kBBytes = (kStN / 8) * kBSbo;                    // 32768
+constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
+constexpr size_t kSolveTcSmem = 2 * size_t(kStageBytes) + 64;
+static_assert(kSolveTcSmem <= 232448, "shared memory of the tensor-core solve");
+static_assert(kASbo % 16 == 0 && kABytes % 16 == 0, "descriptor alignment");
+
+enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
+
+template <int MODE>
+__global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) {
+  constexpr bool kTrans = MODE == kModeBwdGemm || MODE == kModeBwdLinv;
+  constexpr bool kInv = MODE == kModeFwdLinv || MODE == kModeBwdLinv;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * kStageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+  const PanelTask tk = g.tasks[blockIdx.x];
+  const int b = blockIdx.y / g.nchunk;
+  const int j0 = (blockIdx.y % g.nchunk) * kStN;
+  const int kc = min(kStN, g.k - j0);
+  const int np = (kc + 15) & ~15;
+  const DevSym& S = g.S;
+  const int s = tk.s;
+  const int N = S.front_n[s], first = S.sn_first[s];
+  const int ns = S.sn_first[s + 1] - first;
+  const int k0 = tk.p, k1 = tk.t1;
+  const int m0 = tk.t0 * kTcM;
+  const int32_t* rows = S.rows + S.rows_ptr[s];
+  const int mvalid = min(kTcM, (MODE == kModeFwdBnd ? N - ns : ns) - m0);
+  // A source: column-major, leading dimension ld; natural A[m][k] =
+  // M[(roff + m) + k ld], transposed A[m][k] = M[(roff + k) + (m0 + m) ld]
+  const float* M;
+  int ld, roff;
+  if constexpr (kInv) {
+    M = g.linv + int64_t(b) * g.linv_stride + g.linv_off[s];
+    ld = ns;
+    roff = kTrans ? 0 : m0;
+  } else {
+    M = g.fronts + int64_t(b) * g.front_stride + S.front_off[s];
+    ld = N;
+    roff = kTrans ? ns : ns + m0;
+  }
+  const float* X = (MODE == kModeFwdLinv || MODE == kModeBwdGemm ? g.A : g.B) +
+                   int64_t(b) * g.n * g.k;
+  float* Y = (MODE == kModeFwdLinv || MODE == kModeBwdGemm ? g.B : g.A) +
+             int64_t(b) * g.n * g.k;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) tmem_alloc(tmem_slot, kStN);
+  if (tid == 0) {
+    mbar_init(&mbar[0]);
+    mbar_init(&mbar[1]);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = umma_idesc_tf32(kTcM, np);
+  const int nst = (k1 - k0 + kStK - 1) / kStK;
+  bool ok = true;
+  for (int st = 0; st < nst; ++st) {
+    const int buf = st & 1;
+    // the ring slot is free once the MMAs of stage st - 2 have completed
+    if (st >= 2) {
+      ok = tc_wait(&mbar[buf], uint32_t((st - 2) >> 1) & 1u, g.status,
+                   DCT_ERR_DEVICE_TIMEOUT, s, b);
+      if (!ok) break;
+    }
+    unsigned char* Ahi = smem_raw + buf * kStageBytes;
+    unsigned char* Alo = Ahi + kABytes;
+    unsigned char* Bhi = Alo + kABytes;
+    unsigned char* Blo = Bhi + kBBytes;
+    const int kb = k0 + st * kStK;
+    const int kw = min(kStK, k1 - kb);
+    {  // A: 128 x 32, 8 values per thread, all loads before the stores
+      constexpr int kPer = (kTcM * kStK / 32) / kWarps;
+      float v[kPer];
+      uint32_t off[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int gi = warp + u * kWarps;
+        int m, kl;
+        if constexpr (kTrans) {
+          m = (gi % (kTcM / 2)) * 2 + (lane >> 4);
+          kl = (gi / (kTcM / 2)) * 16 + (lane & 15);
+        } else {
+          m = (gi % (kTcM / 8)) * 8 + (lane >> 2);
+          kl = (gi / (kTcM / 8)) * 4 + (lane & 3);
+        }
+        const int kg = kb + kl;
+        bool valid = m < mvalid && kl < kw;
+        if constexpr (MODE == kModeFwdLinv) valid = valid && kg <= m0 + m;
+        if constexpr (MODE == kModeBwdLinv) valid = valid && kg >= m0 + m;
+        const int64_t idx = kTrans ? (roff + kg) + int64_t(m0 + m) * ld
+                                   : (roff + m) + int64_t(kg) * ld;
+        v[u] = valid ? __ldg(M + idx) : 0.0f;
+        off[u] = uint32_t(m >> 3) * kASbo + uint32_t(kl >> 2) * kALbo +
+                 uint32_t(m & 7) * 16 + uint32_t(kl & 3) * 4;
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) tc_store_split(Ahi, Alo, off[u], v[u]);
+    }
+    {  // B: right-hand-side rows, (n = rhs, k = row), 8 n x 4 k per instruction
+      const int np8 = np / 8;
+      const int ncm = np8 * (kStK / 4);
+      for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
+        float v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int cm = c0m + warp + u * kWarps;
+          const int n = (cm % np8) * 8 + (lane >> 2), kl = (cm / np8) * 4 + (lane & 3);
+          v[u] = 0.0f;
+          if (cm < ncm && n < kc && kl < kw) {
+            const int kg = kb + kl;
+            const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
+                                                     : int64_t(first + kg);
+            v[u] = X[row * g.k + j0 + n];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int cm = c0m + warp + u * kWarps;
+          if (cm < ncm)
+            tc_store_split(Bhi, Blo,
+                           uint32_t(cm % np8) * kBSbo + uint32_t(cm / np8) * kBLbo +
+                               uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
+                           v[u]);
+        }
+      }
+    }
+    tc_publish_smem();
+    if (tid == 0) {
+      const uint32_t ah = smem_u32(Ahi), al = smem_u32(Alo);
+      const uint32_t bh = smem_u32(Bhi), bl = smem_u32(Blo);
+      for (int kk = 0; kk < (kw + 7) / 8; ++kk) {
+        const uint64_t dah = umma_desc(ah + kk * 2 * kALbo, kALbo, kASbo);
+        const uint64_t dal = umma_desc(al + kk * 2 * kALbo, kALbo, kASbo);
+        const uint64_t dbh = umma_desc(bh + kk * 2 * kBLbo, kBLbo, kBSbo);
+        const uint64_t dbl = umma_desc(bl + kk * 2 * kBLbo, kBLbo, kBSbo);
+        umma_tf32(tmem, dah, dbh, idesc, (st > 0 || kk > 0) ? 1u : 0u);
+        umma_tf32(tmem, dah, dbl, idesc, 1u);
+        umma_tf32(tmem, dal, dbh, idesc, 1u);
+      }
+      umma_commit(&mbar[buf]);
+    }
+  }
+  // the last commit tracks every MMA issued before it
+  if (ok && nst > 0)
+    ok = tc_wait(&mbar[(nst - 1) & 1], uint32_t((nst - 1) >> 1) & 1u, g.status,
+                 DCT_ERR_DEVICE_TIMEOUT, s, b);
+  if (ok && nst > 0) {
+    const int m = (warp & 3) * 32 + lane;
+    float* dst = nullptr;
+    if (m < mvalid) {
+      const int64_t row = MODE == kModeFwdBnd ? int64_t(rows[ns + m0 + m])
+                                              : int64_t(first + m0 + m);
+      dst = Y + row * g.k + j0;
+    }
+    const float sgn = kInv ? 1.0f : -1.0f;
+    const bool vec = (g.k & 3) == 0;   // 16-byte aligned rows
+    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
+      uint32_t v[32];
+      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+      if (dst != nullptr) {
+#pragma unroll
+        for (int c = 0; c < 32; c += 4) {
+          if (vec && cb + c + 4 <= kc) {
+            atomicAdd(reinterpret_cast<float4*>(dst + cb + c),
+                      make_float4(sgn * __uint_as_float(v[c]), sgn * __uint_as_float(v[c + 1]),
+                                  sgn * __uint_as_float(v[c + 2]),
+                                  sgn * __uint_as_float(v[c + 3])));
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              if (cb + c + q < kc) atomicAdd(dst + cb + c + q, sgn * __uint_as_float(v[c + q]));
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kStN);
+}
+
+}  // namespace
+
+cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g0, int64_t count,
+                            int nbatch, cudaStream_t st) {
+  static_assert(kStN == kSolveTcRhs, "right-hand sides per tensor-core CTA");
+  SolveArgs<float> g = g0;
+  g.nchunk = (g.k + kStN - 1) / kStN;
+  dim3 grid(static_cast<unsigned>(count), static_cast<unsigned>(nbatch * g.nchunk));
+  const void* fn = nullptr;
+  switch (kind) {
+    case kFwdLinvTc: fn = reinterpret_cast<const void*>(k_solve_tc<kModeFwdLinv>); break;
+    case kFwdBndTc: fn = reinterpret_cast<const void*>(k_solve_tc<kModeFwdBnd>); break;
+    case kBwdGemmTc: fn = reinterpret_cast<const void*>(k_solve_tc<kModeBwdGemm>); break;
+    case kBwdLinvTc: fn = reinterpret_cast<const void*>(k_solve_tc<kModeBwdLinv>); break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kSolveTcSmem));
+  if (e != cudaSuccess) return e;
+  switch (kind) {
+    case kFwdLinvTc: k_solve_tc<kModeFwdLinv><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
+    case kFwdBndTc: k_solve_tc<kModeFwdBnd><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
+    case kBwdGemmTc: k_solve_tc<kModeBwdGemm><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
+    default: k_solve_tc<kModeBwdLinv><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace dct

@@ -33,6 +33,19 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
          (uint64_t(1) << 46);                 // descriptor version for sm_100
 }
 
+// the same with explicit core-matrix strides (bytes, multiples of 16)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t((saddr >> 4) & 0x3FFF)) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
 // instruction descriptor: D float32, A and B tf32, both K-major, M x N
 __host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(N >> 3) << 17) |

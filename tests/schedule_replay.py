@@ -14,9 +14,10 @@ import numpy as np
 
 PANEL = 64
 UTILE = 64
-(SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, FWD, BWDGEMM, BWDSTEP, FWDSMALL,
- BWDSMALL, PINV, FWDTC, FWDBND, FWDBNDTC, LINVINIT, LINVT, LINVX, FWDLINV,
- BWDLINV) = range(19)
+TCTILE = 128
+(SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, PINV, LINVINIT, LINVT, LINVX,
+ FWDSMALL, FWDLINV, FWDBND, BWDSMALL, BWDGEMM, BWDLINV, FWDLINVTC, FWDBNDTC,
+ BWDGEMMTC, BWDLINVTC) = range(19)
 
 
 class Struct:
@@ -205,8 +206,6 @@ def _task_solve(S, kind, tk, fronts, A, B, dinv):
     ns = S.ns(s)
     first = int(S.sn_first[s])
     F = S.front(fronts, s)
-    c0 = p * PANEL
-    w = min(PANEL, ns - c0)
     rows = S.rows[S.rows_ptr[s]:S.rows_ptr[s + 1]]
     assert rows.size == N
     if kind == FWDSMALL:
@@ -218,29 +217,16 @@ def _task_solve(S, kind, tk, fronts, A, B, dinv):
         assert ns <= PANEL and p == 0
         y = B[first:first + ns] - F[ns:, :ns].T @ A[rows[ns:]]
         A[first:first + ns] = dinv[(s, 0)].T @ y
-    elif kind == FWD:
-        assert ns > PANEL
-        y = dinv[(s, p)] @ A[first + c0:first + c0 + w]
-        if t0 == 0:
-            B[first + c0:first + c0 + w] = y
-            return
-        r0 = c0 + w + (t0 - 1) * PANEL
-        r1 = min(c0 + w + t1 * PANEL, ns)
-        assert r0 < r1 <= ns
-        A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
-    elif kind in (FWDBND, FWDBNDTC):
-        tile = 128 if kind == FWDBNDTC else PANEL
-        r0 = ns + t0 * tile
-        r1 = min(r0 + tile, N)
+    elif kind == FWDBND:
+        r0 = ns + t0 * PANEL
+        r1 = min(r0 + PANEL, N)
         assert ns < r0 + 1 <= r1
         A[rows[r0:r1]] -= F[r0:r1, :ns] @ B[first:first + ns]
-    elif kind == FWDTC:
-        assert ns > PANEL
-        y = B[first + c0:first + c0 + w]          # written by the y launch
-        r0 = c0 + w + t0 * 128
-        r1 = min(r0 + 128, ns)
-        assert r0 < r1
-        A[rows[r0:r1]] -= F[r0:r1, c0:c0 + w] @ y
+    elif kind == BWDGEMM:
+        c0 = p * PANEL
+        w = min(PANEL, ns - c0)
+        assert w > 0
+        B[first + c0:first + c0 + w] -= F[ns:, c0:c0 + w].T @ A[rows[ns:]]
     elif kind == FWDLINV:
         assert ns > PANEL and p == 0
         X = dinv[("linv", s)]
@@ -255,17 +241,33 @@ def _task_solve(S, kind, tk, fronts, A, B, dinv):
         nr = min(PANEL, ns - r0)
         assert nr > 0
         A[first + r0:first + r0 + nr] = X[r0:ns, r0:r0 + nr].T @ B[first + r0:first + ns]
-    elif kind == BWDGEMM:
-        xb = A[rows[ns:]]
-        B[first + c0:first + c0 + w] -= F[ns:, c0:c0 + w].T @ xb
-    elif kind == BWDSTEP:
-        x = dinv[(s, p)].T @ B[first + c0:first + c0 + w]
-        if t0 == p:
-            A[first + c0:first + c0 + w] = x
-            return
-        ci0 = t0 * PANEL
-        assert ci0 + PANEL <= c0
-        B[first + ci0:first + ci0 + PANEL] -= F[c0:c0 + w, ci0:ci0 + PANEL].T @ x
+    elif kind in (FWDLINVTC, FWDBNDTC, BWDGEMMTC, BWDLINVTC):
+        # tensor-core products: 128-row output tile t0, K range [p, t1),
+        # accumulated (other tasks may add to the same rows)
+        assert ns > PANEL
+        k0, k1, m0 = p, t1, t0 * TCTILE
+        assert 0 <= k0 < k1
+        if kind == FWDBNDTC:
+            mr = min(TCTILE, N - ns - m0)
+            assert mr > 0 and k1 <= ns
+            A[rows[ns + m0:ns + m0 + mr]] -= F[ns + m0:ns + m0 + mr, k0:k1] @ B[first + k0:first + k1]
+        elif kind == BWDGEMMTC:
+            mr = min(TCTILE, ns - m0)
+            assert mr > 0 and k1 <= N - ns
+            B[first + m0:first + m0 + mr] -= (F[ns + k0:ns + k1, m0:m0 + mr].T
+                                             @ A[rows[ns + k0:ns + k1]])
+        else:
+            X = dinv[("linv", s)]
+            mr = min(TCTILE, ns - m0)
+            assert mr > 0 and k1 <= ns
+            m = np.arange(m0, m0 + mr)[:, None]
+            k = np.arange(k0, k1)[None, :]
+            if kind == FWDLINVTC:
+                T = np.where(k <= m, X[m0:m0 + mr, k0:k1], 0.0)
+                B[first + m0:first + m0 + mr] += T @ A[first + k0:first + k1]
+            else:
+                T = np.where(k >= m, X[k0:k1, m0:m0 + mr].T, 0.0)
+                A[first + m0:first + m0 + mr] += T @ B[first + k0:first + k1]
     else:
         raise AssertionError(f"unexpected kind {kind}")
 
@@ -275,6 +277,10 @@ def replay_solve(sym, S, fronts, bp, dinv, dtype=0):
     A = np.array(bp, dtype=float, copy=True)
     B = np.zeros_like(A)
     for which in (1, 2):
+        if dtype == 1:
+            # float32 plans clear the destination of the accumulating
+            # tensor-core products before each pass
+            (B if which == 1 else A)[:] = 0.0
         tasks, launches = sym.schedule(dtype, which)
         for kind, lv, first, count, arg in launches:
             chunk = tasks[first:first + count]
