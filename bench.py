@@ -224,7 +224,12 @@ def count_launches(eng):
     for which in range(5):
         _, launches = sym.schedule(code, which)
         nl[which] = int((launches[:, 3] > 0).sum())
-    factor = nl[0] + nl[3] + nl[4] + (1 if code == 1 else 0)
+    # factor: schedule + panel inverses + supernode inverses, the lower-
+    # triangle clearing launched with every large-front scatter, and the
+    # float64 value copy of float32 plans
+    _, fl = sym.schedule(code, 0)
+    nscatter = int(((fl[:, 0] == 1) & (fl[:, 3] > 0)).sum())
+    factor = nl[0] + nscatter + nl[3] + nl[4] + (1 if code == 1 else 0)
     passes = nl[1] + nl[2]
     if code == 0:
         solve = 1 + passes                       # rhs copy + substitution

@@ -138,6 +138,10 @@ int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
 int dct_plan_profile(dct_plan* plan, int32_t enable, int32_t reset);
 int dct_plan_profile_get(dct_plan* plan, int32_t kind, double* ms,
                          int64_t* launches, double* flops, double* bytes);
+/* The profiled launches one by one, in launch order since the last reset:
+ * kind and device milliseconds of the first min(capacity, *count). */
+int dct_plan_profile_log(dct_plan* plan, int64_t capacity, int32_t* kinds,
+                         double* ms, int64_t* count);
 
 /* Reads the device status words (synchronises the stream): the first error
  * code raised by a kernel since the last call, the supernode where it was

@@ -74,6 +74,8 @@ _SIGS = {
     "dct_plan_profile_get": (C.c_int, [_p, _i32, C.POINTER(C.c_double), _pi64,
                                        C.POINTER(C.c_double),
                                        C.POINTER(C.c_double)]),
+    "dct_plan_profile_log": (C.c_int, [_p, _i64, _pi32, C.POINTER(C.c_double),
+                                       _pi64]),
     "dct_check_status": (C.c_int, [_p, _p, _pi32, _pi32,
                                    C.POINTER(C.c_double)]),
     "dct_sigma_values": (C.c_int, [_i64, _p, _p, _p, _i64, _p, _p, _p, _p]),
@@ -245,6 +247,19 @@ class Plan:
                   "dct_plan_profile_get")
             out[name] = (ms.value, n.value, fl.value, by.value)
         return out
+
+    def profile_log(self):
+        """[(kind name, ms)] of every profiled launch, in launch order."""
+        n = C.c_int64(0)
+        check(lib().dct_plan_profile_log(self._h, 0, None, None, C.byref(n)),
+              "dct_plan_profile_log")
+        kinds = np.zeros(max(n.value, 1), np.int32)
+        ms = np.zeros(max(n.value, 1), np.float64)
+        check(lib().dct_plan_profile_log(
+            self._h, n.value, kinds.ctypes.data_as(C.POINTER(C.c_int32)),
+            ms.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)),
+            "dct_plan_profile_log")
+        return [(self.KINDS[k], float(t)) for k, t in zip(kinds[:n.value], ms[:n.value])]
 
     def status(self, stream):
         code, where, res = C.c_int32(0), C.c_int32(0), C.c_double(0.0)

@@ -483,6 +483,8 @@ cudaError_t dct::Profiler::collect() {
     fl[r.kind] += r.flops;
     by[r.kind] += r.bytes;
     n[r.kind] += 1;
+    log_kind.push_back(r.kind);
+    log_ms.push_back(t);
     pool.push_back(r.a);
     pool.push_back(r.b);
   }
@@ -495,6 +497,8 @@ void dct::Profiler::reset() {
     ms[k] = fl[k] = by[k] = 0.0;
     n[k] = 0;
   }
+  log_kind.clear();
+  log_ms.clear();
 }
 
 extern "C" {
@@ -865,6 +869,21 @@ int dct_plan_profile_get(dct_plan* P, int32_t kind, double* ms, int64_t* launche
   if (launches) *launches = P->prof.n[kind];
   if (flops) *flops = P->prof.fl[kind];
   if (bytes) *bytes = P->prof.by[kind];
+  return DCT_OK;
+}
+
+int dct_plan_profile_log(dct_plan* P, int64_t capacity, int32_t* kinds, double* ms,
+                         int64_t* count) {
+  if (!P || !count) return fail(DCT_ERR_ARG, "bad arguments");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  DCT_CUDA(P->prof.collect(), "profile collect");
+  const int64_t n = int64_t(P->prof.log_ms.size());
+  *count = n;
+  for (int64_t i = 0; i < n && i < capacity; ++i) {
+    if (kinds) kinds[i] = P->prof.log_kind[i];
+    if (ms) ms[i] = P->prof.log_ms[i];
+  }
   return DCT_OK;
 }
 

@@ -94,6 +94,8 @@ struct Profiler {
   std::vector<cudaEvent_t> pool;
   double ms[kNumKinds] = {0}, fl[kNumKinds] = {0}, by[kNumKinds] = {0};
   int64_t n[kNumKinds] = {0};
+  std::vector<int> log_kind;     // every collected launch, in launch order
+  std::vector<double> log_ms;
   cudaError_t begin(int kind, double flops, double bytes, cudaStream_t st);
   cudaError_t end(cudaStream_t st);
   cudaError_t collect();

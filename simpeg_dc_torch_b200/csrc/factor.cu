@@ -57,7 +57,6 @@ k_small_front(DevSym S, const PanelTask* __restrict__ tasks, const void* vals,
   const int b = blockIdx.y;
   const int N = S.front_n[s];
   const int ns = S.sn_first[s + 1] - S.sn_first[s];
-  T* dsh = F + N * N;
   const int tid = threadIdx.x;
   T* out = fronts + int64_t(b) * front_stride + S.front_off[s];
 
@@ -82,30 +81,67 @@ k_small_front(DevSym S, const PanelTask* __restrict__ tasks, const void* vals,
     }
     __syncthreads();
   }
-  // right-looking partial Cholesky of the first ns columns
+  // (1) the ns pivot columns: right-looking, updates confined to the panel
+  //     (rows below k, columns k+1 .. ns-1); each thread owns whole rows
   for (int k = 0; k < ns; ++k) {
     T piv = F[k + k * N];
-    if (!good_pivot(piv)) {
-      if (tid == 0) flag_pivot(status, s, b);
-      piv = T(1);
-    }
+    const bool bad = !good_pivot(piv);
+    if (bad) piv = T(1);
     const T d = sqrt(piv);
     const T inv = T(1) / d;
-    if (tid == 0) dsh[k] = d;
-    const int m = N - k - 1;
-    for (int i = tid; i < m; i += blockDim.x) F[(k + 1 + i) + k * N] *= inv;
+    for (int r = k + 1 + tid; r < N; r += blockDim.x) F[r + k * N] *= inv;
     __syncthreads();
-    for (int idx = tid; idx < m * m; idx += blockDim.x) {
-      const int ii = idx % m, jj = idx / m;
-      if (ii >= jj)
-        F[(k + 1 + ii) + (k + 1 + jj) * N] -=
-            F[(k + 1 + ii) + k * N] * F[(k + 1 + jj) + k * N];
+    if (tid == 0) {
+      F[k + k * N] = d;
+      if (bad) flag_pivot(status, s, b);
+    }
+    for (int r = k + 1 + tid; r < N; r += blockDim.x) {
+      const T lrk = F[r + k * N];
+      const int cmax = min(r, ns - 1);
+      for (int c = k + 1; c <= cmax; ++c) F[r + c * N] -= lrk * F[c + k * N];
     }
     __syncthreads();
   }
-  for (int k = tid; k < ns; k += blockDim.x) F[k + k * N] = dsh[k];
+  // (2) Schur complement of the boundary rows, F_BB -= L_B L_B^T, in 64 x 64
+  //     register tiles (4 x 4 per thread) of the lower triangle
+  const int nbr = N - ns;
+  const int jg = tid & 15, ag = tid >> 4;
+  for (int ti = 0; ti * 64 < nbr; ++ti)
+    for (int tj = 0; tj <= ti; ++tj) {
+      T acc[4][4];
+      zero_acc(acc);
+      int ra[4], rb[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        ra[p] = min(ns + ti * 64 + ag + 16 * p, N - 1);
+        rb[p] = min(ns + tj * 64 + jg + 16 * p, N - 1);
+      }
+      for (int k = 0; k < ns; ++k) {
+        T x[4], y[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          x[p] = F[ra[p] + k * N];
+          y[p] = F[rb[p] + k * N];
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p][q] += x[p] * y[q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = ti * 64 + ag + 16 * p, j = tj * 64 + jg + 16 * q;
+          if (i < nbr && j <= i) F[(ns + i) + (ns + j) * N] -= acc[p][q];
+        }
+    }
   __syncthreads();
-  for (int i = tid; i < N * N; i += blockDim.x) out[i] = F[i];
+  // the whole front, upper part as zeros, so the buffer needs no clearing
+  for (int i = tid; i < N * N; i += blockDim.x) {
+    const int r = i % N, c = i / N;
+    out[i] = r >= c ? F[i] : T(0);
+  }
 }
 
 // ------------------------------------------------------------ large: setup
@@ -121,6 +157,25 @@ k_large_scatter(DevSym S, const PanelTask* __restrict__ tasks, const void* vals,
   for (int64_t q = a0 + threadIdx.x; q < a1; q += blockDim.x)
     F[S.amap_pos[q]] = load_val<T>(vals, vals_dtype,
                                    int64_t(b) * vals_stride + S.amap_e[q]);
+}
+
+// Zero the lower triangle (diagonal included) of the large fronts of a
+// level before their entries are scattered; the upper triangle of a front is
+// never read, and single-CTA fronts write all of theirs.  kZeroSplit CTAs
+// per front, one column per warp at a time.
+constexpr int kZeroSplit = 32;
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_zero_lower(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
+             int64_t front_stride) {
+  const int s = tasks[blockIdx.x].s;
+  const int b = blockIdx.y / kZeroSplit, part = blockIdx.y % kZeroSplit;
+  const int N = S.front_n[s];
+  T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kW = kThreads / 32;
+  for (int c = part * kW + warp; c < N; c += kZeroSplit * kW)
+    for (int r = c + lane; r < N; r += 32) F[r + int64_t(c) * N] = T(0);
 }
 
 // task: s = parent, t0 = child, t1 = first column of the child's update
@@ -162,76 +217,170 @@ k_large_extend_add(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 }
 
 // ------------------------------------------------------------ large: panels
-// Factor the w x w diagonal block D (column-major, ld 64) in shared memory.
-template <typename T>
-__device__ void potrf_smem(T* D, int w, T* dsh, int* status, int s, int b) {
-  const int tid = threadIdx.x;
-  for (int k = 0; k < w; ++k) {
-    T piv = D[k + k * kPanel];
-    if (!good_pivot(piv)) {
-      if (tid == 0) flag_pivot(status, s, b);
-      piv = T(1);
+// Blocked Cholesky D = L L^T of a 64 x 64 diagonal block and X = L^{-1}, in
+// shared memory (ld kDLD, padded so that row and column walks are both free
+// of bank conflicts), over four 16-column block steps kb:
+//   (a) one warp factors D_kk (16 x 16) in registers with shuffles and forms
+//       its inverse X_kk (forward substitution, one column per lane);
+//   (b) all threads: L_rk = D_rk X_kk^T for the rows below, and block row kb
+//       of X, X_kj = X_kk R_kj (j < kb), R being the right-hand side of the
+//       elimination on [L | I] kept in X's storage;
+//   (c) all threads: D_rc -= L_rk L_ck^T (trailing lower triangle) and
+//       R_rj -= L_rk X_kj (j <= kb).
+// Blocks narrower than 64 are padded with the identity.  With FACTOR false
+// D already holds L and only X is formed.  A non-positive or non-finite pivot
+// is flagged and replaced by 1.
+constexpr int kDLD = kPanel + 1;
+constexpr int kDiagSmemElems = 2 * kPanel * kDLD;
+
+template <typename T, int NT, bool FACTOR>
+__device__ __forceinline__ void diag_chol_inv(T* D, T* X, int* status, int s, int b) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int kb = 0; kb < 4; ++kb) {
+    const int o = kb * 16;
+    if (warp == 0) {   // (a)
+      const int i = lane & 15;
+      T v[16];
+      T myr = T(0);   // 1 / L[i, i], held by lane i
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = D[(o + i) + (o + q) * kDLD];
+      if constexpr (FACTOR) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          T piv = __shfl_sync(0xffffffffu, v[k], k);
+          const bool bad = !good_pivot(piv);
+          if (bad) piv = T(1);
+          const T dk = sqrt(piv);
+          const T rk = T(1) / dk;
+          if (bad && lane == 0) flag_pivot(status, s, b);
+          if (i > k) v[k] *= rk;
+          if (i == k) {
+            v[k] = dk;
+            myr = rk;
+          }
+#pragma unroll
+          for (int j = k + 1; j < 16; ++j) {
+            const T ljk = __shfl_sync(0xffffffffu, v[k], j);
+            if (i >= j) v[j] -= v[k] * ljk;
+          }
+        }
+        if (lane < 16) {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) D[(o + i) + (o + q) * kDLD] = q <= i ? v[q] : T(0);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+          if (i == k) myr = T(1) / v[k];
+      }
+      // column j = lane of X_kk: x_i = (delta_ij - sum_{q<i} L_iq x_q) / L_ii
+      T x[16];
+#pragma unroll
+      for (int ii = 0; ii < 16; ++ii) {
+        T acc = (ii == i) ? T(1) : T(0);
+#pragma unroll
+        for (int q = 0; q < ii; ++q) acc -= __shfl_sync(0xffffffffu, v[q], ii) * x[q];
+        x[ii] = acc * __shfl_sync(0xffffffffu, myr, ii);
+      }
+      if (lane < 16) {
+#pragma unroll
+        for (int ii = 0; ii < 16; ++ii) X[(o + ii) + (o + i) * kDLD] = x[ii];
+      }
     }
-    const T d = sqrt(piv);
-    const T inv = T(1) / d;
-    if (tid == 0) dsh[k] = d;
-    const int m = w - k - 1;
-    for (int i = tid; i < m; i += blockDim.x) D[(k + 1 + i) + k * kPanel] *= inv;
     __syncthreads();
-    for (int idx = tid; idx < m * m; idx += blockDim.x) {
-      const int ii = idx % m, jj = idx / m;
-      if (ii >= jj)
-        D[(k + 1 + ii) + (k + 1 + jj) * kPanel] -=
-            D[(k + 1 + ii) + k * kPanel] * D[(k + 1 + jj) + k * kPanel];
+    // (b) L_rk for rows r >= o + 16, and X_kj = X_kk R_kj for j < kb; the
+    //     results overwrite their inputs, so they are staged in registers
+    //     and stored after a barrier
+    {
+      const int nrow = kPanel - o - 16;
+      const int nl = FACTOR ? nrow * 16 : 0, nx = 16 * o;   // nl + nx <= 768
+      constexpr int kMax = (48 * 16 + NT - 1) / NT;
+      T val[kMax];
+#pragma unroll
+      for (int u = 0; u < kMax; ++u) {
+        const int e = tid + u * NT;
+        T acc = T(0);
+        if (e < nl) {
+          const int r = o + 16 + e % nrow, c = e / nrow;
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc += D[r + (o + q) * kDLD] * X[(o + c) + (o + q) * kDLD];
+        } else if (e < nl + nx) {
+          const int f = e - nl, r = f % 16, c = f / 16;   // X[o + r, c], c < o
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc += X[(o + r) + (o + q) * kDLD] * X[(o + q) + c * kDLD];
+        }
+        val[u] = acc;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < kMax; ++u) {
+        const int e = tid + u * NT;
+        if (e < nl) {
+          const int r = o + 16 + e % nrow, c = e / nrow;
+          D[r + (o + c) * kDLD] = val[u];
+        } else if (e < nl + nx) {
+          const int f = e - nl;
+          X[(o + f % 16) + (f / 16) * kDLD] = val[u];
+        }
+      }
+    }
+    __syncthreads();
+    // (c) trailing updates with block column kb of L and block row kb of X
+    {
+      const int t0 = o + 16, nt = kPanel - t0;
+      const int nd = FACTOR ? nt * nt : 0, nr = nt * (o + 16);
+      for (int e = tid; e < nd + nr; e += NT) {
+        if (e < nd) {
+          const int r = t0 + e % nt, c = t0 + e / nt;
+          if (c > r) continue;
+          T acc = T(0);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc += D[r + (o + q) * kDLD] * D[c + (o + q) * kDLD];
+          D[r + c * kDLD] -= acc;
+        } else {
+          const int f = e - nd, r = t0 + f % nt, c = f / nt;
+          T acc = T(0);
+#pragma unroll
+          for (int q = 0; q < 16; ++q) acc += D[r + (o + q) * kDLD] * X[(o + q) + c * kDLD];
+          X[r + c * kDLD] -= acc;
+        }
+      }
     }
     __syncthreads();
   }
-  for (int k = tid; k < w; k += blockDim.x) D[k + k * kPanel] = dsh[k];
-  __syncthreads();
 }
 
-// X = D^{-1} for the factored lower block D (both ld 64): one thread per
-// column j runs the forward substitution D x = e_j.
-template <typename T>
-__device__ void trinv_smem(const T* D, int w, T* X) {
-  const int j = threadIdx.x;
-  if (j < w) {
-    for (int i = 0; i < j; ++i) X[i + j * kPanel] = T(0);
-    X[j + j * kPanel] = T(1) / D[j + j * kPanel];
-    for (int i = j + 1; i < w; ++i) {
-      T acc = T(0);
-      for (int q = j; q < i; ++q) acc += D[i + q * kPanel] * X[q + j * kPanel];
-      X[i + j * kPanel] = -acc / D[i + i * kPanel];
-    }
+// D (and X = I) from the w x w block at rows/columns c0 of the front F
+// (order N), lower part, padded to 64 with the identity
+template <typename T, int NT>
+__device__ __forceinline__ void diag_load(const T* F, int N, int c0, int w, T* D, T* X) {
+  for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += NT) {
+    const int r = idx & 63, c = idx >> 6;
+    T v = (r == c) ? T(1) : T(0);
+    if (r < w && c < w && r >= c) v = F[(c0 + r) + int64_t(c0 + c) * N];
+    D[r + c * kDLD] = v;
+    X[r + c * kDLD] = (r == c) ? T(1) : T(0);
   }
   __syncthreads();
 }
 
 // Factor the diagonal block of the panel starting at column c0 (width w) of
-// front F (order N): L_pp is written back into F (lower part) and D_p^{-1}
-// (w x w, ld w) to `inv`.  Needs kDiagSmemElems elements of shared memory.
-constexpr int kDiagSmemElems = 2 * kPanel * kPanel + kPanel;
-template <typename T>
-__device__ void factor_diag(T* F, int N, int c0, int w, T* sm, T* inv,
-                            int* status, int s, int b) {
+// front F (order N) with NT threads: L_pp is written back into F (lower
+// part) and D_p^{-1} (w x w, ld w) to `inv`.  Needs kDiagSmemElems elements
+// of shared memory at sm.
+template <typename T, int NT>
+__device__ __forceinline__ void factor_diag(T* F, int N, int c0, int w, T* sm, T* inv,
+                                            int* status, int s, int b) {
   T* D = sm;
-  T* X = sm + kPanel * kPanel;
-  T* dsh = X + kPanel * kPanel;
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-    const int r = idx % kPanel, c = idx / kPanel;
-    D[idx] = (r < w && c < w && r >= c) ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
-  }
-  __syncthreads();
-  potrf_smem(D, w, dsh, status, s, b);
-  for (int idx = tid; idx < w * w; idx += blockDim.x) {
-    const int r = idx % w, c = idx / w;
-    if (r >= c) F[(c0 + r) + int64_t(c0 + c) * N] = D[r + c * kPanel];
-  }
-  trinv_smem(D, w, X);
-  for (int idx = tid; idx < w * w; idx += blockDim.x) {
-    const int r = idx % w, c = idx / w;
-    inv[r + c * w] = X[r + c * kPanel];
+  T* X = sm + kPanel * kDLD;
+  diag_load<T, NT>(F, N, c0, w, D, X);
+  diag_chol_inv<T, NT, true>(D, X, status, s, b);
+  for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += NT) {
+    const int r = idx & 63, c = idx >> 6;
+    if (r < w && c < w) {
+      if (r >= c) F[(c0 + r) + int64_t(c0 + c) * N] = D[r + c * kDLD];
+      inv[r + c * w] = X[r + c * kDLD];
+    }
   }
 }
 
@@ -288,7 +437,7 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 constexpr int kUT = kUpdateTile;
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
                int64_t front_stride, T* dinv, const int64_t* dinv_off,
                int64_t dinv_stride, int* status) {
@@ -307,7 +456,7 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   T* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
   const int tid = threadIdx.x;
   if (tk.t0 < 0) {
-    factor_diag(F, N, c0, w, As, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
+    factor_diag<T, kThreads>(F, N, c0, w, As, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
     return;
   }
   const int ri = base + tk.t0 * kUT, rj = base + tk.t1 * kUT;
@@ -343,7 +492,7 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
     }
   if (tk.t0 == 0 && tk.t1 == 0 && base < ns) {
     __syncthreads();   // this CTA's updates of the block are complete
-    factor_diag(F, N, base, min(kPanel, ns - base), As,
+    factor_diag<T, kThreads>(F, N, base, min(kPanel, ns - base), As,
                 Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
   }
 }
@@ -421,7 +570,8 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   float* sm = reinterpret_cast<float*>(base_ptr);
   if (tk.t0 < 0) {
-    factor_diag(F, N, c0, w, sm, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
+    factor_diag<float, kTcThreads>(F, N, c0, w, sm, Dv + int64_t(tk.p) * kPanel * kPanel, status, s,
+                                    b);
     return;
   }
   const int ri = base + tk.t0 * kTcM, rj = base + tk.t1 * kTcN;
@@ -458,7 +608,7 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   if (warp == 0) tmem_dealloc(tmem, kTcN);
   if (done && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
     __syncthreads();   // this CTA's updates of the block are complete
-    factor_diag(F, N, base, min(kPanel, ns - base), sm,
+    factor_diag<float, kTcThreads>(F, N, base, min(kPanel, ns - base), sm,
                 Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
   }
 }
@@ -475,8 +625,8 @@ k_panel_inverse(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
                 int64_t front_stride, T* dinv, const int64_t* dinv_off,
                 int64_t dinv_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* L = reinterpret_cast<T*>(smem_raw);       // ld kPanel
-  T* X = L + kPanel * kPanel;                   // ld kPanel
+  T* L = reinterpret_cast<T*>(smem_raw);       // ld kDLD
+  T* X = L + kPanel * kDLD;                     // ld kDLD
   const PanelTask tk = tasks[blockIdx.x];
   const int b = blockIdx.y;
   const int s = tk.s;
@@ -485,16 +635,12 @@ k_panel_inverse(DevSym S, const PanelTask* __restrict__ tasks, const T* fronts,
   const int c0 = tk.p * kPanel;
   const int w = min(kPanel, ns - c0);
   const T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-    const int r = idx % w, c = idx / w;
-    L[r + c * kPanel] = r >= c ? F[(c0 + r) + int64_t(c0 + c) * N] : T(0);
-  }
-  __syncthreads();
-  trinv_smem(L, w, X);
+  diag_load<T, kThreads>(F, N, c0, w, L, X);
+  diag_chol_inv<T, kThreads, false>(L, X, nullptr, s, b);
   T* out = dinv + int64_t(b) * dinv_stride + dinv_off[s] + int64_t(tk.p) * kPanel * kPanel;
   for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
     const int r = idx % w, c = idx / w;
-    out[r + c * w] = X[r + c * kPanel];
+    out[r + c * w] = X[r + c * kDLD];
   }
 }
 
@@ -657,15 +803,14 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                         int64_t vals_stride, cudaStream_t st) {
   T* fronts = static_cast<T*>(P->fronts);
   const int nb = P->nbatch;
-  cudaError_t e = cudaMemsetAsync(fronts, 0,
-                                  sizeof(T) * P->front_stride * size_t(nb), st);
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
   const int small_max = sizeof(T) == 8 ? kSmallFrontF64 : kSmallFrontF32;
   const size_t small_smem = sizeof(T) * (size_t(small_max) * small_max + small_max);
   const size_t panel_smem = sizeof(T) * (2 * kPanel * kPanel);
-  // the update kernel's tiles, or factor_diag's D, X and pivots, whichever is larger
-  static_assert(2 * kPanel * kUT + kPanel >= kDiagSmemElems, "update smem too small");
-  const size_t update_smem = sizeof(T) * (2 * kPanel * kUT + kPanel);
+  // the update kernel's tiles, or factor_diag's D and X, whichever is larger
+  constexpr int kUpdateElems =
+      2 * kPanel * kUT > kDiagSmemElems ? 2 * kPanel * kUT : kDiagSmemElems;
+  const size_t update_smem = sizeof(T) * kUpdateElems;
   // attributes are per device: set them on every call (cheap host calls)
   e = cudaFuncSetAttribute(k_small_front<T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -701,6 +846,8 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
         break;
       }
       case kLargeScatter:
+        k_zero_lower<T><<<dim3(static_cast<unsigned>(L.count), nb * kZeroSplit), kThreads,
+                          0, st>>>(P->ds, t, fronts, P->front_stride);
         k_large_scatter<T><<<grid, kThreads, 0, st>>>(
             P->ds, t, vals, vals_dtype, vals_stride, fronts, P->front_stride);
         break;
@@ -735,7 +882,7 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
   }
   // inverses of the diagonal blocks of small fronts, for the substitution
   // (large fronts store theirs while factoring)
-  const size_t inv_smem = sizeof(T) * 2 * kPanel * kPanel;
+  const size_t inv_smem = sizeof(T) * kDiagSmemElems;
   e = cudaFuncSetAttribute(k_panel_inverse<T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(inv_smem));
