@@ -230,6 +230,20 @@ k_large_extend_add(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 // Blocks narrower than 64 are padded with the identity.  With FACTOR false
 // D already holds L and only X is formed.  A non-positive or non-finite pivot
 // is flagged and replaced by 1.
+// 1/sqrt(x) for x > 0: the hardware reciprocal square root estimate in
+// float, then Newton-Raphson steps y <- y (3 - x y^2) / 2 (each doubles the
+// correct bits; one for float, three for double from the float estimate).
+__device__ __forceinline__ float inv_sqrt(float x) {
+  float y = rsqrtf(x);
+  return y * (1.5f - 0.5f * x * y * y);
+}
+__device__ __forceinline__ double inv_sqrt(double x) {
+  double y = double(rsqrtf(float(x)));
+#pragma unroll
+  for (int it = 0; it < 3; ++it) y = y * (1.5 - 0.5 * x * y * y);
+  return y;
+}
+
 constexpr int kDLD = kPanel + 1;
 constexpr int kDiagSmemElems = 2 * kPanel * kDLD;
 
@@ -250,8 +264,8 @@ __device__ __forceinline__ void diag_chol_inv(T* D, T* X, int* status, int s, in
           T piv = __shfl_sync(0xffffffffu, v[k], k);
           const bool bad = !good_pivot(piv);
           if (bad) piv = T(1);
-          const T dk = sqrt(piv);
-          const T rk = T(1) / dk;
+          const T rk = inv_sqrt(piv);
+          const T dk = piv * rk;
           if (bad && lane == 0) flag_pivot(status, s, b);
           if (i > k) v[k] *= rk;
           if (i == k) {
@@ -369,7 +383,7 @@ __device__ __forceinline__ void diag_load(const T* F, int N, int c0, int w, T* D
 // part) and D_p^{-1} (w x w, ld w) to `inv`.  Needs kDiagSmemElems elements
 // of shared memory at sm.
 template <typename T, int NT>
-__device__ __forceinline__ void factor_diag(T* F, int N, int c0, int w, T* sm, T* inv,
+__device__ __noinline__ void factor_diag(T* F, int N, int c0, int w, T* sm, T* inv,
                                             int* status, int s, int b) {
   T* D = sm;
   T* X = sm + kPanel * kDLD;

@@ -135,32 +135,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
 #pragma unroll
       for (int u = 0; u < kPer; ++u) tc_store_split(Ahi, Alo, off[u], v[u]);
     }
-    {  // B: right-hand-side rows, (n = rhs, k = row), 8 n x 4 k per instruction
-      const int np8 = np / 8;
-      const int ncm = np8 * (kStK / 4);
-      for (int c0m = 0; c0m < ncm; c0m += 16 * kWarps) {
-        float v[16];
+    {  // B: right-hand-side rows, (n = rhs, k = row), 8 n x 4 k per warp
+       // instruction; the layout always has kStN / 8 groups of n (compile-
+       // time index math), groups at or beyond np are never read by the MMA
+      constexpr int kNG = kStN / 8;
+      constexpr int kPer = kNG * (kStK / 4) / kWarps;
+      float v[kPer];
+      int64_t row[kPer];
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int cm = c0m + warp + u * kWarps;
-          const int n = (cm % np8) * 8 + (lane >> 2), kl = (cm / np8) * 4 + (lane & 3);
-          v[u] = 0.0f;
-          if (cm < ncm && n < kc && kl < kw) {
-            const int kg = kb + kl;
-            const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
-                                                     : int64_t(first + kg);
-            v[u] = X[row * g.k + j0 + n];
-          }
-        }
+      for (int u = 0; u < kPer; ++u) {
+        const int cm = warp + u * kWarps;
+        const int kl = (cm / kNG) * 4 + (lane & 3);
+        const int kg = kb + min(kl, kw - 1);
+        row[u] = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg)) : int64_t(first + kg);
+      }
 #pragma unroll
-        for (int u = 0; u < 16; ++u) {
-          const int cm = c0m + warp + u * kWarps;
-          if (cm < ncm)
-            tc_store_split(Bhi, Blo,
-                           uint32_t(cm % np8) * kBSbo + uint32_t(cm / np8) * kBLbo +
-                               uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
-                           v[u]);
-        }
+      for (int u = 0; u < kPer; ++u) {
+        const int cm = warp + u * kWarps;
+        const int n = (cm % kNG) * 8 + (lane >> 2), kl = (cm / kNG) * 4 + (lane & 3);
+        v[u] = (n < kc && kl < kw) ? X[row[u] * g.k + j0 + n] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; ++u) {
+        const int cm = warp + u * kWarps;
+        if ((cm % kNG) * 8 < np)
+          tc_store_split(Bhi, Blo,
+                         uint32_t(cm % kNG) * kBSbo + uint32_t(cm / kNG) * kBLbo +
+                             uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
+                         v[u]);
       }
     }
     tc_publish_smem();
