@@ -93,6 +93,55 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   const uint32_t idesc = umma_idesc_tf32(kTcM, np);
   const int nst = (k1 - k0 + kStK - 1) / kStK;
   bool ok = true;
+  // operand registers: stage st + 1 is loaded while the MMAs of stage st run
+  constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 8
+  constexpr int kNG = kStN / 8;                               // n groups of B
+  constexpr int kPerB = kNG * (kStK / 4) / kWarps;            // 16
+  float va[kPerA], vb[kPerB];
+  // element (m, kl) of A handled in slot u (fixed over the stages)
+  auto a_coord = [&](int u, int& m, int& kl) {
+    const int gi = warp + u * kWarps;
+    if constexpr (kTrans) {
+      m = (gi % (kTcM / 2)) * 2 + (lane >> 4);
+      kl = (gi / (kTcM / 2)) * 16 + (lane & 15);
+    } else {
+      m = (gi % (kTcM / 8)) * 8 + (lane >> 2);
+      kl = (gi / (kTcM / 8)) * 4 + (lane & 3);
+    }
+  };
+  auto load_stage = [&](int st) {
+    const int kb = k0 + st * kStK;
+    const int kw = min(kStK, k1 - kb);
+#pragma unroll
+    for (int u = 0; u < kPerA; ++u) {
+      int m, kl;
+      a_coord(u, m, kl);
+      const int kg = kb + kl;
+      bool valid = m < mvalid && kl < kw;
+      if constexpr (MODE == kModeFwdLinv) valid = valid && kg <= m0 + m;
+      if constexpr (MODE == kModeBwdLinv) valid = valid && kg >= m0 + m;
+      const int64_t idx = kTrans ? (roff + kg) + int64_t(m0 + m) * ld
+                                 : (roff + m) + int64_t(kg) * ld;
+      va[u] = valid ? __ldg(M + idx) : 0.0f;
+    }
+    // B: right-hand-side rows (n = rhs, k = row), 8 n x 4 k per warp
+    // instruction; kStN / 8 groups of n always (compile-time index math)
+    int64_t row[kPerB];
+#pragma unroll
+    for (int u = 0; u < kPerB; ++u) {
+      const int cm = warp + u * kWarps;
+      const int kl = (cm / kNG) * 4 + (lane & 3);
+      const int kg = kb + min(kl, kw - 1);
+      row[u] = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg)) : int64_t(first + kg);
+    }
+#pragma unroll
+    for (int u = 0; u < kPerB; ++u) {
+      const int cm = warp + u * kWarps;
+      const int n = (cm % kNG) * 8 + (lane >> 2), kl = (cm / kNG) * 4 + (lane & 3);
+      vb[u] = (n < kc && kl < kw) ? X[row[u] * g.k + j0 + n] : 0.0f;
+    }
+  };
+  if (nst > 0) load_stage(0);
   for (int st = 0; st < nst; ++st) {
     const int buf = st & 1;
     // the ring slot is free once the MMAs of stage st - 2 have completed
@@ -105,66 +154,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
     unsigned char* Alo = Ahi + kABytes;
     unsigned char* Bhi = Alo + kABytes;
     unsigned char* Blo = Bhi + kBBytes;
-    const int kb = k0 + st * kStK;
-    const int kw = min(kStK, k1 - kb);
-    {  // A: 128 x 32, 8 values per thread, all loads before the stores
-      constexpr int kPer = (kTcM * kStK / 32) / kWarps;
-      float v[kPer];
-      uint32_t off[kPer];
+    const int kw = min(kStK, k1 - (k0 + st * kStK));
 #pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int gi = warp + u * kWarps;
-        int m, kl;
-        if constexpr (kTrans) {
-          m = (gi % (kTcM / 2)) * 2 + (lane >> 4);
-          kl = (gi / (kTcM / 2)) * 16 + (lane & 15);
-        } else {
-          m = (gi % (kTcM / 8)) * 8 + (lane >> 2);
-          kl = (gi / (kTcM / 8)) * 4 + (lane & 3);
-        }
-        const int kg = kb + kl;
-        bool valid = m < mvalid && kl < kw;
-        if constexpr (MODE == kModeFwdLinv) valid = valid && kg <= m0 + m;
-        if constexpr (MODE == kModeBwdLinv) valid = valid && kg >= m0 + m;
-        const int64_t idx = kTrans ? (roff + kg) + int64_t(m0 + m) * ld
-                                   : (roff + m) + int64_t(kg) * ld;
-        v[u] = valid ? __ldg(M + idx) : 0.0f;
-        off[u] = uint32_t(m >> 3) * kASbo + uint32_t(kl >> 2) * kALbo +
-                 uint32_t(m & 7) * 16 + uint32_t(kl & 3) * 4;
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) tc_store_split(Ahi, Alo, off[u], v[u]);
+    for (int u = 0; u < kPerA; ++u) {
+      int m, kl;
+      a_coord(u, m, kl);
+      tc_store_split(Ahi, Alo,
+                     uint32_t(m >> 3) * kASbo + uint32_t(kl >> 2) * kALbo +
+                         uint32_t(m & 7) * 16 + uint32_t(kl & 3) * 4,
+                     va[u]);
     }
-    {  // B: right-hand-side rows, (n = rhs, k = row), 8 n x 4 k per warp
-       // instruction; the layout always has kStN / 8 groups of n (compile-
-       // time index math), groups at or beyond np are never read by the MMA
-      constexpr int kNG = kStN / 8;
-      constexpr int kPer = kNG * (kStK / 4) / kWarps;
-      float v[kPer];
-      int64_t row[kPer];
 #pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int cm = warp + u * kWarps;
-        const int kl = (cm / kNG) * 4 + (lane & 3);
-        const int kg = kb + min(kl, kw - 1);
-        row[u] = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg)) : int64_t(first + kg);
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int cm = warp + u * kWarps;
-        const int n = (cm % kNG) * 8 + (lane >> 2), kl = (cm / kNG) * 4 + (lane & 3);
-        v[u] = (n < kc && kl < kw) ? X[row[u] * g.k + j0 + n] : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; ++u) {
-        const int cm = warp + u * kWarps;
-        if ((cm % kNG) * 8 < np)
-          tc_store_split(Bhi, Blo,
-                         uint32_t(cm % kNG) * kBSbo + uint32_t(cm / kNG) * kBLbo +
-                             uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
-                         v[u]);
-      }
+    for (int u = 0; u < kPerB; ++u) {
+      const int cm = warp + u * kWarps;
+      if ((cm % kNG) * 8 < np)   // groups at or beyond np are never read
+        tc_store_split(Bhi, Blo,
+                       uint32_t(cm % kNG) * kBSbo + uint32_t(cm / kNG) * kBLbo +
+                           uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
+                       vb[u]);
     }
+    if (st + 1 < nst) load_stage(st + 1);
     tc_publish_smem();
     if (tid == 0) {
       const uint32_t ah = smem_u32(Ahi), al = smem_u32(Alo);

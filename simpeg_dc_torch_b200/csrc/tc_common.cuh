@@ -160,13 +160,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Store value v (float) of operand element (m, k) into the hi/lo operands.
+// Store value v (float) of operand element (m, k) into the hi/lo operands:
+// hi = v rounded to TF32, lo = v - hi (exact in float; the tensor core reads
+// its leading 19 bits, so the part of v below both is dropped, ~2^-22 |v|).
 __device__ __forceinline__ void tc_store_split(unsigned char* hi, unsigned char* lo,
                                                uint32_t off, float v) {
   const uint32_t h = tf32_rna(v);
-  const uint32_t l = tf32_rna(v - __uint_as_float(h));
   *reinterpret_cast<uint32_t*>(hi + off) = h;
-  *reinterpret_cast<uint32_t*>(lo + off) = l;
+  *reinterpret_cast<float*>(lo + off) = v - __uint_as_float(h);
 }
 
 }  // namespace dct
