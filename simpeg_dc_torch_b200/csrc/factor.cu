@@ -247,60 +247,67 @@ __device__ __forceinline__ double inv_sqrt(double x) {
 constexpr int kDLD = kPanel + 1;
 constexpr int kDiagSmemElems = 2 * kPanel * kDLD;
 
+// Step (a) of diag_chol_inv for one 16 x 16 diagonal block at offset o:
+// run by one warp only (a separate, non-inlined function so that the other
+// warps branch around it instead of issuing it predicated off).
+template <typename T, bool FACTOR>
+__device__ __noinline__ void diag_leaf16(T* D, T* X, int o, int* status, int s, int b) {
+  const int lane = threadIdx.x & 31;
+  const int i = lane & 15;
+  T v[16];
+  T myr = T(0);   // 1 / L[i, i], held by lane i
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = D[(o + i) + (o + q) * kDLD];
+  if constexpr (FACTOR) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      T piv = __shfl_sync(0xffffffffu, v[k], k);
+      const bool bad = !good_pivot(piv);
+      if (bad) piv = T(1);
+      const T rk = inv_sqrt(piv);
+      const T dk = piv * rk;
+      if (bad && lane == 0) flag_pivot(status, s, b);
+      if (i > k) v[k] *= rk;
+      if (i == k) {
+        v[k] = dk;
+        myr = rk;
+      }
+#pragma unroll
+      for (int j = k + 1; j < 16; ++j) {
+        const T ljk = __shfl_sync(0xffffffffu, v[k], j);
+        if (i >= j) v[j] -= v[k] * ljk;
+      }
+    }
+    if (lane < 16) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) D[(o + i) + (o + q) * kDLD] = q <= i ? v[q] : T(0);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (i == k) myr = T(1) / v[k];
+  }
+  // column j = lane of X_kk: x_i = (delta_ij - sum_{q<i} L_iq x_q) / L_ii
+  T x[16];
+#pragma unroll
+  for (int ii = 0; ii < 16; ++ii) {
+    T acc = (ii == i) ? T(1) : T(0);
+#pragma unroll
+    for (int q = 0; q < ii; ++q) acc -= __shfl_sync(0xffffffffu, v[q], ii) * x[q];
+    x[ii] = acc * __shfl_sync(0xffffffffu, myr, ii);
+  }
+  if (lane < 16) {
+#pragma unroll
+    for (int ii = 0; ii < 16; ++ii) X[(o + ii) + (o + i) * kDLD] = x[ii];
+  }
+}
+
 template <typename T, int NT, bool FACTOR>
 __device__ __forceinline__ void diag_chol_inv(T* D, T* X, int* status, int s, int b) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int kb = 0; kb < 4; ++kb) {
     const int o = kb * 16;
-    if (warp == 0) {   // (a)
-      const int i = lane & 15;
-      T v[16];
-      T myr = T(0);   // 1 / L[i, i], held by lane i
-#pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] = D[(o + i) + (o + q) * kDLD];
-      if constexpr (FACTOR) {
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          T piv = __shfl_sync(0xffffffffu, v[k], k);
-          const bool bad = !good_pivot(piv);
-          if (bad) piv = T(1);
-          const T rk = inv_sqrt(piv);
-          const T dk = piv * rk;
-          if (bad && lane == 0) flag_pivot(status, s, b);
-          if (i > k) v[k] *= rk;
-          if (i == k) {
-            v[k] = dk;
-            myr = rk;
-          }
-#pragma unroll
-          for (int j = k + 1; j < 16; ++j) {
-            const T ljk = __shfl_sync(0xffffffffu, v[k], j);
-            if (i >= j) v[j] -= v[k] * ljk;
-          }
-        }
-        if (lane < 16) {
-#pragma unroll
-          for (int q = 0; q < 16; ++q) D[(o + i) + (o + q) * kDLD] = q <= i ? v[q] : T(0);
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-          if (i == k) myr = T(1) / v[k];
-      }
-      // column j = lane of X_kk: x_i = (delta_ij - sum_{q<i} L_iq x_q) / L_ii
-      T x[16];
-#pragma unroll
-      for (int ii = 0; ii < 16; ++ii) {
-        T acc = (ii == i) ? T(1) : T(0);
-#pragma unroll
-        for (int q = 0; q < ii; ++q) acc -= __shfl_sync(0xffffffffu, v[q], ii) * x[q];
-        x[ii] = acc * __shfl_sync(0xffffffffu, myr, ii);
-      }
-      if (lane < 16) {
-#pragma unroll
-        for (int ii = 0; ii < 16; ++ii) X[(o + ii) + (o + i) * kDLD] = x[ii];
-      }
-    }
+    if (warp == 0) diag_leaf16<T, FACTOR>(D, X, o, status, s, b);   // (a)
     __syncthreads();
     // (b) L_rk for rows r >= o + 16, and X_kj = X_kk R_kj for j < kb; the
     //     results overwrite their inputs, so they are staged in registers
