@@ -427,7 +427,8 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
                 int64_t(tk.p) * kPanel * kPanel;
   const int r0 = c0 + w + (tk.t0 - 1) * kPanel;
   const int nr = min(kPanel, N - r0);
-  for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+#pragma unroll
+  for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += kThreads) {
     const int a = idx % kPanel, q = idx / kPanel;
     S1[idx] = (a < w && q < w) ? Di[a + q * w] : T(0);
     S2[idx] = (a < nr && q < w) ? F[(r0 + a) + int64_t(c0 + q) * N] : T(0);
@@ -482,7 +483,8 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   }
   const int ri = base + tk.t0 * kUT, rj = base + tk.t1 * kUT;
   const int ni = min(kUT, N - ri), nj = min(kUT, N - rj);
-  for (int idx = tid; idx < kPanel * kUT; idx += blockDim.x) {
+#pragma unroll
+  for (int idx = tid; idx < kPanel * kUT; idx += kThreads) {
     const int r = idx % kUT, k = idx / kUT;
     const bool kin = k < w;
     As[idx] = (kin && r < ni) ? F[(ri + r) + int64_t(c0 + k) * N] : T(0);
@@ -721,7 +723,8 @@ k_linv_t(LinvArgs g, const T* fronts, const T* linv, T* ltmp) {
   zero_acc(acc);
   for (int k0 = cc0; k0 < h; k0 += kPanel) {
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += kThreads) {
       const int q = idx % kPanel, c = idx / kPanel;   // q: k index (contiguous)
       S1[q * (kPanel + 1) + c] = X[(a0 + k0 + q) + int64_t(a0 + cc0 + c) * ns];
       const int r = idx % kPanel, kk = idx / kPanel;
@@ -762,7 +765,8 @@ k_linv_x(LinvArgs g, const T* ltmp, T* linv) {
   for (int k0 = 0; k0 <= r0; k0 += kPanel) {
     const int kw = min(kPanel, hd - k0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kPanel * kPanel; idx += kThreads) {
       const int q = idx % kPanel, c = idx / kPanel;
       S1[q * (kPanel + 1) + c] =
           (q < kw) ? Tt[(d0 + k0 + q) + int64_t(a0 + cc0 + c) * ns] : T(0);

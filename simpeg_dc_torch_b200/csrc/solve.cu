@@ -37,6 +37,12 @@ __device__ __forceinline__ void atomic_sub(T* p, T v) {
   atomicAdd(p, -v);
 }
 
+// resident CTAs per SM the CUDA-core substitution kernels are compiled for:
+// their shared memory admits 4 (float) / 2 (double); 3 caps float at 85
+// registers
+template <typename T>
+constexpr int kSolveMinBlocks = sizeof(T) == 4 ? 3 : 2;
+
 // S1 (the "a" operand) uses a padded leading dimension: several loaders
 // store it transposed, which would otherwise hit one bank 32 times.
 constexpr int kLD1 = kLD + 1;
@@ -54,7 +60,8 @@ template <typename T>
 __device__ __forceinline__ void load_rhs(T* S, const T* __restrict__ src, int k,
                                          int j0, int rc, int nr,
                                          const int32_t* map, int64_t r0) {
-  for (int idx = threadIdx.x; idx < kLD * kRC; idx += blockDim.x) {
+#pragma unroll
+  for (int idx = threadIdx.x; idx < kLD * kRC; idx += kThreads) {
     const int r = idx / kRC, j = idx % kRC;
     T v = T(0);
     if (r < nr && j < rc) {
@@ -70,7 +77,8 @@ __device__ __forceinline__ void load_rhs(T* S, const T* __restrict__ src, int k,
 template <typename T>
 __device__ __forceinline__ void load_dinv(T* S, const T* __restrict__ Di, int w,
                                           bool transposed) {
-  for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+  for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
     const int r = idx % kLD, c = idx / kLD;
     const T v = (r < w && c < w) ? Di[r + c * w] : T(0);
     if (transposed) S[r * kLD1 + c] = v;
@@ -81,14 +89,16 @@ __device__ __forceinline__ void load_dinv(T* S, const T* __restrict__ Di, int w,
 // ------------------------------------------------------------ forward, small
 // one CTA: y = D^{-1} b (to B), then b[boundary rows] -= L_B y (atomics, A)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd_small(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_small(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
   T* Y = S2 + kLD * kLD;
-  const int s = g.tasks[blockIdx.x].s;
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  // the right-hand-side chunks of a task are adjacent CTAs (its L block
+  // is then read from HBM once and from L2 by the other chunks)
+  const int s = g.tasks[blockIdx.x / g.nchunk].s;
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int N = S.front_n[s], first = S.sn_first[s];
@@ -115,7 +125,8 @@ __global__ void __launch_bounds__(kThreads) k_fwd_small(SolveArgs<T> g) {
   for (int r0 = w; r0 < N; r0 += kLD) {
     const int nr = min(kLD, N - r0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
       const int r = idx % kLD, c = idx / kLD;
       S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c) * N] : T(0);
     }
@@ -141,13 +152,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_small(SolveArgs<T> g) {
 // boundary rows [ns, N) receives -L[tile, 0:ns] y_s (y_s = all panels, in B),
 // accumulated over the panels before one atomic update per element.
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd_bnd(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_bnd(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const PanelTask tk = g.tasks[blockIdx.x / g.nchunk];
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int s = tk.s;
@@ -164,7 +175,8 @@ __global__ void __launch_bounds__(kThreads) k_fwd_bnd(SolveArgs<T> g) {
   for (int c0 = 0; c0 < ns; c0 += kPanel) {
     const int w = min(kPanel, ns - c0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
       const int r = idx % kLD, c = idx / kLD;
       S1[c * kLD1 + r] = (r < nr && c < w) ? F[(r0 + r) + int64_t(c0 + c) * N] : T(0);
     }
@@ -189,13 +201,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_bnd(SolveArgs<T> g) {
 // ------------------------------------------------------------ inverse products
 // large supernodes: y_s = L_ss^{-1} b_s, 64-row tile t0 per CTA (B <- A rows)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_fwd_linv(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_linv(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[a, k]
   T* S2 = S1 + kLD1 * kLD;                  // [k][j]: b[k, j]
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const PanelTask tk = g.tasks[blockIdx.x / g.nchunk];
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int s = tk.s;
@@ -210,7 +222,8 @@ __global__ void __launch_bounds__(kThreads) k_fwd_linv(SolveArgs<T> g) {
   for (int k0 = 0; k0 <= r0; k0 += kLD) {
     const int kw = min(kLD, ns - k0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
       const int a = idx % kLD, kk = idx / kLD;
       S1[kk * kLD1 + a] = (a < nr && kk < kw) ? X[(r0 + a) + int64_t(k0 + kk) * ns] : T(0);
     }
@@ -230,13 +243,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_linv(SolveArgs<T> g) {
 
 // large supernodes: x_s = L_ss^{-T} y_s, 64-row tile t0 per CTA (A <- B rows)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_bwd_linv(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_linv(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[k, a]
   T* S2 = S1 + kLD1 * kLD;                  // [k][j]: y[k, j]
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const PanelTask tk = g.tasks[blockIdx.x / g.nchunk];
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int s = tk.s;
@@ -251,7 +264,8 @@ __global__ void __launch_bounds__(kThreads) k_bwd_linv(SolveArgs<T> g) {
   for (int k0 = r0; k0 < ns; k0 += kLD) {
     const int kw = min(kLD, ns - k0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
       const int kk = idx % kLD, a = idx / kLD;
       S1[kk * kLD1 + a] = (a < nr && kk < kw) ? X[(k0 + kk) + int64_t(r0 + a) * ns] : T(0);
     }
@@ -278,7 +292,8 @@ __device__ void boundary_product(const T* F, int N, int ns, int c0, int w,
   for (int i0 = ns; i0 < N; i0 += kLD) {
     const int ni = min(kLD, N - i0);
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kLD * kLD; idx += blockDim.x) {
+#pragma unroll
+    for (int idx = threadIdx.x; idx < kLD * kLD; idx += kThreads) {
       const int r = idx % kLD, c = idx / kLD;
       S1[r * kLD1 + c] = (r < ni && c < w) ? F[(i0 + r) + int64_t(c0 + c) * N] : T(0);
     }
@@ -291,14 +306,16 @@ __device__ void boundary_product(const T* F, int N, int ns, int c0, int w,
 // ------------------------------------------------------------ backward, small
 // one CTA: y -= L_B^T x_B ; x = D^{-T} y (to A)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_bwd_small(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_small(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
   T* Y = S2 + kLD * kLD;
-  const int s = g.tasks[blockIdx.x].s;
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  // the right-hand-side chunks of a task are adjacent CTAs (its L block
+  // is then read from HBM once and from L2 by the other chunks)
+  const int s = g.tasks[blockIdx.x / g.nchunk].s;
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int N = S.front_n[s], first = S.sn_first[s];
@@ -335,13 +352,13 @@ __global__ void __launch_bounds__(kThreads) k_bwd_small(SolveArgs<T> g) {
 // ------------------------------------------------------------ backward gemm
 // large supernodes: y_p (B) -= L[boundary rows, panel p]^T x[boundary rows]
 template <typename T>
-__global__ void __launch_bounds__(kThreads) k_bwd_gemm(SolveArgs<T> g) {
+__global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_gemm(SolveArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
-  const PanelTask tk = g.tasks[blockIdx.x];
-  const int b = blockIdx.y / g.nchunk;
-  const int j0 = (blockIdx.y % g.nchunk) * kRC;
+  const PanelTask tk = g.tasks[blockIdx.x / g.nchunk];
+  const int b = blockIdx.y;
+  const int j0 = (blockIdx.x % g.nchunk) * kRC;
   const int rc = min(kRC, g.k - j0);
   const DevSym& S = g.S;
   const int s = tk.s;
@@ -500,7 +517,7 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
           cudaSuccess)
         return e;
       g.tasks = sc->d_tasks + L.first;
-      dim3 grid(static_cast<unsigned>(L.count), P->nbatch * nchunk);
+      dim3 grid(static_cast<unsigned>(L.count * nchunk), P->nbatch);
       switch (L.kind) {
         case kFwdSmall: k_fwd_small<T><<<grid, kThreads, smem3, st>>>(g); break;
         case kFwdBnd: k_fwd_bnd<T><<<grid, kThreads, smem3, st>>>(g); break;
