@@ -120,7 +120,8 @@ int dct_solve(dct_plan* plan, const void* d_b, int32_t io_dtype,
 
 /* The same solve on float64 buffers already in permuted order:
  * d_bp (n, k) shared or (nbatch, n, k); d_xp (nbatch, n, k).  d_bp may alias
- * d_xp only when batched.  Used by the fused engine paths. */
+ * d_xp only when batched and only in float64 plans (a float32 plan forms its
+ * refinement residuals from d_bp).  Used by the fused engine paths. */
 int dct_solve_permuted(dct_plan* plan, const double* d_bp, int32_t b_batched,
                        int32_t k, double* d_xp, void* stream);
 
@@ -205,6 +206,44 @@ int dct_gather_contract_plain(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
                               const int32_t* d_row, const int32_t* d_col,
                               int32_t dtype, const void* d_Y, const void* d_X,
                               void* d_gv, void* stream);
+
+/* ---- linearised products of the 2.5-D engine (float64) ------------------- */
+
+/* y = M x for a CSR matrix with int64 row pointers: the value perturbation
+ * dvals = L (-sigma v) of a Jacobian-vector product.  Replaces
+ * torch.sparse.mm(eng.Lstack, ...) in Linearization2D.Jvec
+ * (dctorch/simulation2d.py:692-694). */
+int dct_csr_spmv(int64_t nrows, const int64_t* d_ptr, const int32_t* d_col,
+                 const double* d_val, const double* d_x, double* d_y, void* stream);
+
+/* Y_b[iperm[i], :] = alpha * sum_e vals_b[e] X_b[iperm[col_e], :] over row i
+ * of the pattern (crow/col in user order, X/Y permuted (nbatch, n, k),
+ * X != Y): the right-hand sides -A_k(dvals) U_k.  Replaces the per-ky CSR
+ * products of Linearization2D.Jvec (dctorch/simulation2d.py:697-703). */
+int dct_pattern_spmm(int32_t nbatch, int32_t n, int32_t k, const int32_t* d_crow,
+                     const int32_t* d_col, const int32_t* d_iperm, const double* d_vals,
+                     int64_t nnz, double alpha, const double* d_X, double* d_Y,
+                     void* stream);
+
+/* gv[(b*nnz + e)*nb + r] = -scale[b] Y_b[iperm row_e, r] U_b[iperm col_e, sidx[r]]:
+ * one adjoint column per datum contracted with that datum's own source field
+ * (Y permuted (nbatch, n, nb), U permuted (nbatch, n, ns)).  Replaces the
+ * per-ky gathers of TorchDC2D.Jmatrix (dctorch/simulation2d.py:502-505) and
+ * Linearization2D._grad_vals_pairwise (808-818). */
+int dct_gather_pairwise(int32_t nbatch, int64_t n, int64_t nnz, int32_t nb, int32_t ns,
+                        const int32_t* d_row, const int32_t* d_col,
+                        const int32_t* d_iperm, const double* d_scale,
+                        const int32_t* d_sidx, const double* d_Y, const double* d_U,
+                        double* d_gv, void* stream);
+
+/* out[c, r] = -sigma[c] sum_q Lt_val[q] gv[Lt_col[q], r] for nb columns
+ * (out (nC, nb), gv (rows of L, nb)): rows of the Jacobian through L^T.
+ * Replaces torch.sparse.mm(Lstack.t(), ...) of TorchDC2D.Jmatrix
+ * (dctorch/simulation2d.py:506-507) and Linearization2D._Lt (659-674). */
+int dct_values_vjp_multi(int64_t nC, int32_t nb, const int64_t* d_Lt_ptr,
+                         const int32_t* d_Lt_col, const double* d_Lt_val,
+                         const double* d_sigma, const double* d_gv, double* d_out,
+                         void* stream);
 
 /* ---- allocation-free small solve -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

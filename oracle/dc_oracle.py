@@ -148,6 +148,46 @@ def jtvec_2d(op, m, v):
     return _adjoint_2d(op, m, np.asarray(v, float))[1]
 
 
+def jvec_2d(op, m, u):
+    """J u for J = d(dpred)/dm (simulation2d.py:526-529 through
+    Linearization2D.Jvec, 689-710): A_k dU_k = -A_k(dsigma) U_k with
+    dsigma = -sigma u, then J u = (Pd sum_k wq_k dU_k)[i, sidx_i]."""
+    nky = len(op["wq"])
+    d, VALS, slv, U = dpred_2d(op, m, return_fields=True)
+    dvals = (op["Lstack"] @ (-sigma_of(m) * np.asarray(u, float))).reshape(nky, -1)
+    n = op["nN"]
+    rhs = np.stack([-(sp.csr_matrix((dvals[k], op["col"], op["crow"]),
+                                    shape=(n, n)) @ U[k]) for k in range(nky)])
+    dU = slv.solve(rhs)
+    dbar = np.tensordot(op["wq"], dU, axes=(0, 0))
+    PU = op["Pd"] @ dbar
+    return PU[np.arange(PU.shape[0]), op["sidx"]]
+
+
+def jmatrix_2d(op, m):
+    """The explicit (nD, nC) sensitivity matrix (simulation2d.py:439-518):
+    Y_k = A_k^{-1} Pd^T (one column per datum r);
+    J[r] = -sigma * L^T (-wq_k Y_k[row_e, r] U_k[col_e, sidx_r])."""
+    nky = len(op["wq"])
+    d, VALS, slv, U = dpred_2d(op, m, return_fields=True)
+    Y = slv.solve(op["Pd"].T.toarray())            # (nky, nN, nD)
+    r = row_of(op["crow"])
+    c = op["col"]
+    sidx = op["sidx"]
+    nD = op["Pd"].shape[0]
+    gv = np.empty((nky, len(c), nD))
+    for k in range(nky):
+        gv[k] = -op["wq"][k] * Y[k][r] * U[k][c][:, sidx]
+    J = op["Lstack"].T @ gv.reshape(nky * len(c), nD)  # (nC, nD)
+    return (-sigma_of(m)[:, None] * J).T
+
+
+def diag_jtdj_2d(op, m, dw):
+    """diag(J^T diag(dw) J) (simulation2d.py:778-793)."""
+    J = jmatrix_2d(op, m)
+    return (J ** 2).T @ np.asarray(dw, float)
+
+
 # ------------------------------------------------------------------- 3-D
 def dpred_3d(op, m, return_fields=False):
     """simulation3d.py:197-207: VALS = L3 exp(-m); U = A^{-1} q; d = (Pd U)[i, sidx]."""

@@ -6,7 +6,7 @@ reference's solver and engine interfaces:
 
     make_solver, make_batch_solver, DCTSolver, DCTBatchSolver,
     sparse_solve, sparse_solve_batch, sparse_solve_batch_prefactored,
-    TorchDC2D, TorchDC3D
+    TorchDC2D, TorchDC3D, Linearization2D
 
 Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
 discretize / SimPEG objects, which may be passed instead.
@@ -19,5 +19,5 @@ from .survey import (DipoleReceiver, DipoleSource, PoleReceiver,  # noqa: F401
 from .solver import (CuDSSBatchSolver, CuDSSSolver, DCTBatchSolver,  # noqa: F401
                      DCTSolver, make_batch_solver, make_solver, sparse_solve,
                      sparse_solve_batch, sparse_solve_batch_prefactored)
-from .simulation2d import TorchDC2D  # noqa: F401
+from .simulation2d import Linearization2D, TorchDC2D  # noqa: F401
 from .simulation3d import TorchDC3D  # noqa: F401

@@ -74,6 +74,7 @@ class FusedPath:
         iperm = np.empty_like(perm)
         iperm[perm] = np.arange(perm.size, dtype=perm.dtype)
         self.iperm_host = iperm
+        self.iperm_d = torch.as_tensor(iperm.astype(np.int64), device=device)
         self.L_ptr, self.L_col, self.L_val = _csr64(L, device)
         self.Lt_ptr, self.Lt_col, self.Lt_val = _csr64(sp.csr_matrix(L.T), device)
         self.w = None if w is None else torch.as_tensor(
@@ -90,6 +91,10 @@ class FusedPath:
         self.Pd_ptr = torch.as_tensor(Pd.indptr.astype(np.int32), device=device)
         self.Pd_col = torch.as_tensor(Pd.indices.astype(np.int32), device=device)
         self.Pd_val = torch.as_tensor(Pd.data.astype(np.float64), device=device)
+        self.Pd_indptr = Pd.indptr.astype(np.int64)
+        self.Pd_row = torch.as_tensor(
+            np.repeat(np.arange(Pd.shape[0]), np.diff(Pd.indptr)).astype(np.int64),
+            device=device)
         self.sidx = np.asarray(sidx, dtype=np.int64)
         self.sidx_d = torch.as_tensor(self.sidx.astype(np.int32), device=device)
         groups = {}
@@ -200,6 +205,59 @@ class FusedPath:
             self.Lt_val.data_ptr(), sigma.data_ptr(), gv.data_ptr(),
             gm.data_ptr(), self._st()), "dct_values_vjp")
         return gm
+
+
+    # ------------------------------------------------ linearised products
+    def jvec(self, v_full, sigma, U):
+        """J v (nD,) on the current factorization and fields U:
+        A_k dU_k = -A_k(dvals) U_k with dvals = L (-sigma v), then the
+        weighted projection of dU (dctorch/simulation2d.py:689-710)."""
+        x = (-sigma * v_full.to(self.device, torch.float64)).contiguous()
+        dvals = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
+                            device=self.device)
+        nat.check(nat.lib().dct_csr_spmv(
+            dvals.numel(), self.L_ptr.data_ptr(), self.L_col.data_ptr(),
+            self.L_val.data_ptr(), x.data_ptr(), dvals.data_ptr(), self._st()),
+            "dct_csr_spmv")
+        k = U.shape[-1]
+        rhs = torch.empty_like(U)
+        nat.check(nat.lib().dct_pattern_spmm(
+            self.nbatch, self.nN, k, self.solver.crow.data_ptr(),
+            self.col_e.data_ptr(), self._iperm_ptr, dvals.data_ptr(),
+            self.nnzA, -1.0, U.data_ptr(), rhs.data_ptr(), self._st()),
+            "dct_pattern_spmm")
+        self._plan.set_refinement(self.refine_fields)
+        dU = torch.empty_like(rhs)
+        self._plan.solve_permuted(rhs.data_ptr(), 1, k, dU.data_ptr(), self._st())
+        return self.project(dU)
+
+    def jac_block(self, a, b, sigma, U):
+        """Rows a..b of the Jacobian w.r.t. m_full as an (nC, b - a) block:
+        one adjoint solve with the columns a..b of Pd^T and the pairwise
+        contraction with each datum's own source field
+        (dctorch/simulation2d.py:439-518, 727-776)."""
+        nb = b - a
+        p0, p1 = int(self.Pd_indptr[a]), int(self.Pd_indptr[b])
+        rhs = torch.zeros((self.nN, nb), dtype=torch.float64, device=self.device)
+        rhs.index_put_((self.iperm_d[self.Pd_col[p0:p1].long()],
+                        self.Pd_row[p0:p1] - a), self.Pd_val[p0:p1],
+                       accumulate=True)
+        self._plan.set_refinement(self.refine_adj)
+        Y = self._solve_perm(rhs, nb)
+        gv = torch.empty((self.nbatch * self.nnzA, nb), dtype=torch.float64,
+                         device=self.device)
+        nat.check(nat.lib().dct_gather_pairwise(
+            self.nbatch, self.nN, self.nnzA, nb, U.shape[-1],
+            self.row_e.data_ptr(), self.col_e.data_ptr(), self._iperm_ptr,
+            None if self.w is None else self.w.data_ptr(),
+            self.sidx_d[a:b].contiguous().data_ptr(), Y.data_ptr(), U.data_ptr(),
+            gv.data_ptr(), self._st()), "dct_gather_pairwise")
+        Jb = torch.empty((self.nC, nb), dtype=torch.float64, device=self.device)
+        nat.check(nat.lib().dct_values_vjp_multi(
+            self.nC, nb, self.Lt_ptr.data_ptr(), self.Lt_col.data_ptr(),
+            self.Lt_val.data_ptr(), sigma.data_ptr(), gv.data_ptr(),
+            Jb.data_ptr(), self._st()), "dct_values_vjp_multi")
+        return Jb
 
 
 class FusedDpred(torch.autograd.Function):

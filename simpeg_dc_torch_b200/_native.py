@@ -89,6 +89,12 @@ _SIGS = {
     "dct_gather_contract_plain": (C.c_int, [_i32, _i64, _i64, _i32, _p, _p,
                                             _i32, _p, _p, _p, _p]),
     "dct_solve_small_noalloc": (C.c_int, [_i32, _p, _p, _p, _p, _i32, _p, _p]),
+    "dct_csr_spmv": (C.c_int, [_i64, _p, _p, _p, _p, _p, _p]),
+    "dct_pattern_spmm": (C.c_int, [_i32, _i32, _i32, _p, _p, _p, _p, _i64,
+                                   C.c_double, _p, _p, _p]),
+    "dct_gather_pairwise": (C.c_int, [_i32, _i64, _i64, _i32, _i32, _p, _p, _p,
+                                      _p, _p, _p, _p, _p, _p]),
+    "dct_values_vjp_multi": (C.c_int, [_i64, _i32, _p, _p, _p, _p, _p, _p, _p]),
 }
 
 

@@ -799,6 +799,9 @@ int dct_solve_permuted(dct_plan* P, const double* d_bp, int32_t b_batched,
   if (!P || !d_bp || !d_xp || k < 1 || k > P->max_rhs)
     return fail(DCT_ERR_ARG, "bad arguments");
   if (!P->factored) return fail(DCT_ERR_NOT_FACTORED, "solve before factorize");
+  if (P->dtype == DCT_F32 && d_bp == d_xp)
+    return fail(DCT_ERR_ARG, "float32 plans refine against the right-hand side: "
+                             "d_bp must not alias d_xp");
   int rc = set_device(P->device);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

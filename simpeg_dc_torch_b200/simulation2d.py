@@ -56,6 +56,11 @@ class _ActiveCells:
     def full(self, m):
         return self.v.to(m.dtype).index_add(0, self.idx, m)
 
+    def inject(self, v):
+        """P v: a perturbation of the active cells on the full mesh."""
+        out = torch.zeros(self.v.numel(), dtype=v.dtype, device=v.device)
+        return out.index_add(0, self.idx, v)
+
     def restrict(self, g_full):
         return g_full[self.idx]
 
@@ -201,6 +206,132 @@ class TorchDC2D:
             g = self._path.adjoint(v.reshape(-1), U, sigma)
         return self._grad_to_model(g, m)
 
+    # ------------------------------------------------ linearised products
+    def _jac_rows(self, sigma, U, a, b):
+        """Rows a..b of J as an (nM, b - a) block (active cells only)."""
+        Jb = self._path.jac_block(a, b, sigma, U)
+        return Jb if self._inj is None else Jb[self._inj.idx]
+
+    def Jmatrix(self, m, block=32):
+        """The explicit (nD, nM) Jacobian from one factorization
+        (dctorch/simulation2d.py:439-518): the adjoint right-hand sides are the
+        columns of Pd^T, solved `block` data at a time on the same factors.
+        Returned outside the autograd graph on m's device and dtype."""
+        block = max(1, min(int(block), self.nD, self._path.width))
+        with torch.no_grad():
+            m_full = self._model_to_full(m)
+            _, sigma, U, _ = self._path.forward(m_full)
+            J = torch.empty((self.nD, self._nM()), dtype=torch.float64,
+                            device=self.device)
+            for a in range(0, self.nD, block):
+                b = min(a + block, self.nD)
+                J[a:b] = self._jac_rows(sigma, U, a, b).T
+        return J.to(device=m.device, dtype=m.dtype)
+
+    def linearize(self, m, store_fields=None, fields_max_gib=2.0):
+        """The forward frozen at m: one factorization, the fields kept, and
+        J v / J^T v as one batched solve each (see `Linearization2D`)."""
+        return Linearization2D(self, m, store_fields=store_fields,
+                               fields_max_gib=fields_max_gib)
+
+    def Jvec(self, m, v):
+        """J v without forming J (dctorch/simulation2d.py:526-529)."""
+        return self.linearize(m).Jvec(v)
+
+    def _nM(self):
+        return self.nC if self._inj is None else self._inj.nA
+
     def check(self):
         """Synchronise and raise if a kernel reported an error."""
         return self.solver.check()
+
+
+class Linearization2D:
+    """The 2.5-D forward frozen at one model, for Gauss-Newton
+    (dctorch/simulation2d.py:537-818).
+
+    The systems are factorized once and the fields U_k = A_k^{-1} q are kept
+    on the device (when they fit `fields_max_gib`, otherwise re-solved from
+    the stored factors for each product).  Then
+
+        J v   :  A_k dU_k = -A_k(dsigma) U_k, dsigma = -sigma v;  J v = Pd sum_k w_k dU_k
+        J^T v :  A_k Y_k = Pd^T v on the same factors; contraction with U_k, L^T, -sigma
+
+    each one batched solve over all wavenumbers and sources.  `diag_JtDJ` and
+    `Jmatrix` form rows of J `sub` data at a time (one adjoint solve per
+    block) and never hold more than one block.  The solver is shared with the
+    engine: if anything else refactorizes it (a line-search `dpred`), its
+    stamp changes and this factorization is restored before the next product.
+    """
+
+    def __init__(self, eng, m, store_fields=None, fields_max_gib=2.0):
+        self.eng = eng
+        self.m_dtype, self.m_device = m.dtype, m.device
+        path = eng._path
+        with torch.no_grad():
+            self.m_full = eng._model_to_full(m)
+            self.sigma, self.vals = path.values(self.m_full)
+            path.factorize(self.vals)
+            self._stamp = path.solver.stamp
+            U = path.fields()
+            self.d = path.project(U).to(self.m_device, self.m_dtype)
+        nbytes = U.numel() * U.element_size()
+        if store_fields is None:
+            store_fields = nbytes <= fields_max_gib * 2 ** 30
+        self._U = U if store_fields else None
+        self.width = path.width
+
+    def _ensure(self):
+        path = self.eng._path
+        if path.solver.stamp != self._stamp:
+            path.factorize(self.vals)
+            self._stamp = path.solver.stamp
+
+    def _fields(self):
+        self._ensure()
+        return self._U if self._U is not None else self.eng._path.fields()
+
+    def _v_full(self, v):
+        v = v.to(self.eng.device, torch.float64).reshape(-1)
+        return v if self.eng._inj is None else self.eng._inj.inject(v)
+
+    def _out(self, x):
+        return x.to(self.m_device, self.m_dtype)
+
+    @torch.no_grad()
+    def Jvec(self, v):
+        """J v, (nD,)."""
+        U = self._fields()
+        return self._out(self.eng._path.jvec(self._v_full(v), self.sigma, U))
+
+    @torch.no_grad()
+    def Jtvec(self, v):
+        """J^T v, (nM,)."""
+        U = self._fields()
+        g = self.eng._path.adjoint(v.reshape(-1), U, self.sigma)
+        return self._out(g if self.eng._inj is None else self.eng._inj.restrict(g))
+
+    def _blocks(self, sub):
+        nb = self.width if not sub else max(1, min(int(sub), self.width))
+        U = self._fields()
+        for a in range(0, self.eng.nD, nb):
+            b = min(a + nb, self.eng.nD)
+            yield a, b, self.eng._jac_rows(self.sigma, U, a, b)
+
+    @torch.no_grad()
+    def diag_JtDJ(self, dw, sub=None):
+        """diag(J^T diag(dw) J), (nM,), exact, without storing J."""
+        dw = dw.to(self.eng.device, torch.float64).reshape(-1)
+        out = torch.zeros(self.eng._nM(), dtype=torch.float64, device=self.eng.device)
+        for a, b, Jb in self._blocks(sub):
+            out += (Jb ** 2) @ dw[a:b]
+        return self._out(out)
+
+    @torch.no_grad()
+    def Jmatrix(self, sub=None):
+        """The explicit J (nD, nM) from this linearization's factors and fields."""
+        J = torch.empty((self.eng.nD, self.eng._nM()), dtype=torch.float64,
+                        device=self.eng.device)
+        for a, b, Jb in self._blocks(sub):
+            J[a:b] = Jb.T
+        return self._out(J)

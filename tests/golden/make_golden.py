@@ -20,6 +20,8 @@ path in float64:
       misfit_and_grad from TorchDC2D.
   dc2d_suite.npz  : the reference suite's 2-D tensor case
       (dctorch/tests/test_suite.py:65-67), outputs + operator checksums.
+  dc2d_lin.npz    : on the dc2d_tiny problem, TorchDC2D.Jmatrix and Jvec,
+      and Linearization2D's d, Jvec, Jtvec, diag_JtDJ and Jmatrix.
   dc3d_tiny.npz / dc3d_suite.npz : the same for TorchDC3D.
 """
 from __future__ import annotations
@@ -212,6 +214,31 @@ def main():
                        Pd_data=ops.Pd.data, sidx=ops.sidx)
         np.savez_compressed(os.path.join(out, name + ".npz"), **rec)
         print(name, "nN", ops.nN, "nD", ops.nD, "nky", len(kys))
+
+    # linearised products of the 2.5-D engine on the tiny problem (its
+    # operators are stored in dc2d_tiny.npz): TorchDC2D.Jmatrix / Jvec and
+    # Linearization2D.Jvec / Jtvec / diag_JtDJ / Jmatrix
+    mesh, survey, m = syn.tiny_2d()
+    ops = nodal_operators(mesh, survey)
+    rmin, rmax = electrode_distance_range(survey)
+    kys, wq, _ = Q.k0_quadrature(rmin, rmax, 7)
+    eng, _ = engine_2d(S2, ops, kys, wq)
+    rng = np.random.default_rng(23)
+    u = rng.standard_normal(ops.nC)
+    v = rng.standard_normal(ops.nD)
+    dw = rng.uniform(0.5, 2.0, ops.nD)
+    mt = torch.tensor(m)
+    rec = dict(m=m, u=u, v=v, dw=dw)
+    rec["jmatrix"] = eng.Jmatrix(mt, block=5).numpy()
+    rec["jvec"] = eng.Jvec(mt, torch.tensor(u)).numpy()
+    lin = eng.linearize(mt)
+    rec["lin_d"] = lin.d.numpy()
+    rec["lin_jvec"] = lin.Jvec(torch.tensor(u)).numpy()
+    rec["lin_jtvec"] = lin.Jtvec(torch.tensor(v)).numpy()
+    rec["lin_diag"] = lin.diag_JtDJ(torch.tensor(dw), sub=3).numpy()
+    rec["lin_jmatrix"] = lin.Jmatrix(sub=4).numpy()
+    np.savez_compressed(os.path.join(out, "dc2d_lin.npz"), **rec)
+    print("dc2d_lin", rec["jmatrix"].shape)
 
     for name, (mesh, survey, m), store_ops in [
             ("dc3d_tiny", syn.tiny_3d(), True),

@@ -69,3 +69,24 @@ def test_oracle_gradient_is_a_derivative():
     fd = (O.misfit_2d(op, m + h * u, dobs, w)
           - O.misfit_2d(op, m - h * u, dobs, w)) / (2 * h)
     assert abs(fd - grad @ u) <= 1e-6 * abs(fd)
+
+
+def test_linearised_products_match_reference():
+    """Jmatrix / Jvec / diag(J^T D J) of the oracle against the reference's
+    TorchDC2D.Jmatrix, Jvec and Linearization2D (dctorch/simulation2d.py:
+    439-529, 537-818), run on the dc2d_tiny problem."""
+    g = golden("dc2d_tiny")
+    L = golden("dc2d_lin")
+    op = _ops(g, False)
+    m = L["m"]
+    J = O.jmatrix_2d(op, m)
+    assert O.rel(J, L["jmatrix"]) < 1e-11
+    assert O.rel(J, L["lin_jmatrix"]) < 1e-11
+    assert O.rel(O.jvec_2d(op, m, L["u"]), L["jvec"]) < 1e-11
+    assert O.rel(L["lin_jvec"], L["jvec"]) < 1e-12
+    assert O.rel(O.jtvec_2d(op, m, L["v"]), L["lin_jtvec"]) < 1e-11
+    assert O.rel(O.diag_jtdj_2d(op, m, L["dw"]), L["lin_diag"]) < 1e-11
+    assert O.rel(O.dpred_2d(op, m), L["lin_d"]) < 1e-12
+    # J is the Jacobian of dpred: its rows are the Jtvec of unit data
+    u = L["u"]
+    assert O.rel(J @ u, L["jvec"]) < 1e-11
