@@ -58,18 +58,6 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
   return r;
 }
 
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, P1;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
 __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1u));
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -126,13 +114,33 @@ __device__ __forceinline__ void umma_3xtf32(uint32_t tmem, uint32_t a_hi, uint32
       : "memory");
 }
 
+// try_wait that may suspend the thread for up to kTcSuspendNs while the phase
+// is incomplete (it returns as soon as the phase completes)
+constexpr uint32_t kTcSuspendNs = 2000;
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(kTcSuspendNs)
+      : "memory");
+  return ok != 0;
+}
+
 // All threads: bounded wait for phase `parity` of the mbarrier; the result is
-// the same in every thread of the CTA.  On timeout the first error is flagged.
+// the same in every thread of the CTA.  Only warp 0 polls (the other warps
+// wait at the CTA barrier and issue nothing); at most kTcWaitLimit polls of
+// at most kTcSuspendNs each.  On timeout the first error is flagged.
 __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* status,
                                         int code, int s, int b) {
-  bool done = false;
-  for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it)
-    done = mbar_try_wait(smem_u32(bar), parity);
+  bool done = true;
+  if (threadIdx.x < 32) {
+    done = false;
+    for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it)
+      done = mbar_try_wait_sleep(smem_u32(bar), parity);
+  }
   done = __syncthreads_and(done) != 0;
   if (!done && threadIdx.x == 0) {
     if (atomicCAS(&status[0], 0, code) == 0) {
