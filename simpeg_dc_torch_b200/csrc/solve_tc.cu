@@ -33,12 +33,16 @@ constexpr int kWarps = kTcThreads / 32;
 // ones (8 rows x 4 K) both store to 32 distinct banks.
 constexpr uint32_t kALbo = 160, kASbo = 7 * kALbo + 128;      // 1248
 constexpr int kABytes = (kTcM / 8) * kASbo;                    // 19968
-constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo;   // 1024
-constexpr int kBBytes = (kStN / 8) * kBSbo;                    // 32768
+// B operand (32 K x 256 N), K-major: N-groups of 8 kBSbo = 1040 B apart (one
+// 16 B slot of skew per group, so that the scalar stores of a warp that holds
+// 8 consecutive float4 along N for 4 rows hit distinct banks)
+constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo + 16;   // 1040
+constexpr int kBBytes = (kStN / 8) * kBSbo;                         // 33280
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
 constexpr size_t kSolveTcSmem = 2 * size_t(kStageBytes) + 64;
 static_assert(kSolveTcSmem <= 232448, "shared memory of the tensor-core solve");
-static_assert(kASbo % 16 == 0 && kABytes % 16 == 0, "descriptor alignment");
+static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
+                  kBBytes % 16 == 0, "descriptor alignment");
 
 enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
 
@@ -95,9 +99,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   bool ok = true;
   // operand registers: stage st + 1 is loaded while the MMAs of stage st run
   constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 8
-  constexpr int kNG = kStN / 8;                               // n groups of B
-  constexpr int kPerB = kNG * (kStK / 4) / kWarps;            // 16
-  float va[kPerA], vb[kPerB];
+  constexpr int kPerB = kStN * kStK / 4 / kTcThreads;        // 4 float4
+  float va[kPerA];
+  float4 vb[kPerB];
+  const bool vec4 = (g.k & 3) == 0;   // 16-byte aligned rows
+  // quad u of this thread: rows kl = 4 (warp-chunk) + lane % 4, quads
+  // n = 4 (8 (chunk) + lane / 4); 64 chunks of 4 rows x 32 columns
+  auto b_coord = [&](int u, int& n, int& kl) {
+    const int c = warp + u * kWarps;           // 0 .. 63
+    kl = (c / 8) * 4 + (lane & 3);
+    n = ((c % 8) * 8 + (lane >> 2)) * 4;
+  };
   // element (m, kl) of A handled in slot u (fixed over the stages)
   auto a_coord = [&](int u, int& m, int& kl) {
     const int gi = warp + u * kWarps;
@@ -124,21 +136,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
                                  : (roff + m) + int64_t(kg) * ld;
       va[u] = valid ? __ldg(M + idx) : 0.0f;
     }
-    // B: right-hand-side rows (n = rhs, k = row), 8 n x 4 k per warp
-    // instruction; kStN / 8 groups of n always (compile-time index math)
-    int64_t row[kPerB];
+    // B: 4 consecutive right-hand sides of one row per slot (a float4 when
+    // the rows are 16-byte aligned); a warp holds 8 consecutive quads of N
+    // (32 right-hand sides) for 4 consecutive rows
 #pragma unroll
     for (int u = 0; u < kPerB; ++u) {
-      const int cm = warp + u * kWarps;
-      const int kl = (cm / kNG) * 4 + (lane & 3);
-      const int kg = kb + min(kl, kw - 1);
-      row[u] = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg)) : int64_t(first + kg);
-    }
-#pragma unroll
-    for (int u = 0; u < kPerB; ++u) {
-      const int cm = warp + u * kWarps;
-      const int n = (cm % kNG) * 8 + (lane >> 2), kl = (cm / kNG) * 4 + (lane & 3);
-      vb[u] = (n < kc && kl < kw) ? X[row[u] * g.k + j0 + n] : 0.0f;
+      int n, kl;
+      b_coord(u, n, kl);
+      float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (kl < kw && n < kc) {
+        const int kg = kb + kl;
+        const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
+                                                 : int64_t(first + kg);
+        const float* src = X + row * g.k + j0 + n;
+        if (vec4 && n + 4 <= kc) {
+          val = *reinterpret_cast<const float4*>(src);
+        } else {
+          val.x = src[0];
+          if (n + 1 < kc) val.y = src[1];
+          if (n + 2 < kc) val.z = src[2];
+          if (n + 3 < kc) val.w = src[3];
+        }
+      }
+      vb[u] = val;
     }
   };
   if (nst > 0) load_stage(0);
@@ -166,12 +186,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
     }
 #pragma unroll
     for (int u = 0; u < kPerB; ++u) {
-      const int cm = warp + u * kWarps;
-      if ((cm % kNG) * 8 < np)   // groups at or beyond np are never read
-        tc_store_split(Bhi, Blo,
-                       uint32_t(cm % kNG) * kBSbo + uint32_t(cm / kNG) * kBLbo +
-                           uint32_t(lane >> 2) * 16 + uint32_t(lane & 3) * 4,
-                       vb[u]);
+      int n, kl;
+      b_coord(u, n, kl);
+      if (n < np) {   // columns at or beyond np are never read
+        const float vv[4] = {vb[u].x, vb[u].y, vb[u].z, vb[u].w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int nq = n + q;
+          tc_store_split(Bhi, Blo,
+                         uint32_t(nq >> 3) * kBSbo + uint32_t(kl >> 2) * kBLbo +
+                             uint32_t(nq & 7) * 16 + uint32_t(kl & 3) * 4,
+                         vv[q]);
+        }
+      }
     }
     if (st + 1 < nst) load_stage(st + 1);
     tc_publish_smem();
