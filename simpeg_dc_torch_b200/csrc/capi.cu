@@ -286,7 +286,26 @@ void push_split(std::vector<PanelTask>& T, int s, int t, int k0, int k1) {
 void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
                            dct::Schedule* bwd) {
   const bool tc = dtype == DCT_F32;
-  auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel; };
+  // Single-panel supernodes run in one CTA each (k_fwd_small / k_bwd_small),
+  // except in float32 plans whose single-panel fronts are mostly large (at
+  // least kTcSmallFront rows hold most of their substitution work, as in 3-D
+  // grids): there they all take the tensor-core products with every right-
+  // hand side in one CTA.  For small fronts (2-D grids) a one-CTA-per-SM
+  // tensor-core task costs more than it saves.
+  constexpr int kTcSmallFront = 128;
+  bool small_tc = false;
+  if (tc) {
+    double big = 0, all = 0;
+    for (int s = 0; s < S.nsuper; ++s) {
+      const double ns = S.ns(s), nb = S.nb(s);
+      if (ns > dct::kPanel) continue;
+      const double wk = ns * ns + 2 * nb * ns;
+      all += wk;
+      if (S.front_n[s] >= kTcSmallFront) big += wk;
+    }
+    small_tc = all > 0 && big >= 0.5 * all;
+  }
+  auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel && !small_tc; };
   auto add = [&](dct::Schedule* sc, int kind, int lv, auto&& fill) {
     Launch l{kind, lv, int64_t(sc->tasks.size()), 0, 0};
     fill(sc->tasks);
@@ -365,14 +384,18 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
 // runs two launches over every pair of blocks: T = C A^{-1}, then
 // X = -D^{-1} T, on 64 x 64 output tiles (t0 = tile row, t1 = tile column,
 // p = pair index, launch arg = h).  Offsets: ns^2 elements per supernode.
-void build_linv_schedule(const dct::Symbolic& S, dct::Schedule* sc,
+// Float32 plans keep an inverse for every supernode (single-panel ones too:
+// their substitution runs on the same tensor-core products); float64 plans
+// only for supernodes wider than one panel.
+void build_linv_schedule(const dct::Symbolic& S, int dtype, dct::Schedule* sc,
                          std::vector<int64_t>* off, int64_t* total) {
+  const int min_ns = dtype == DCT_F32 ? 1 : dct::kPanel + 1;
   off->assign(S.nsuper, -1);
   int64_t acc = 0;
   int max_ns = 0;
   for (int s = 0; s < S.nsuper; ++s) {
     const int ns = S.ns(s);
-    if (ns <= dct::kPanel) continue;
+    if (ns < min_ns) continue;
     (*off)[s] = acc;
     acc += int64_t(ns) * ns;
     max_ns = std::max(max_ns, ns);
@@ -381,7 +404,7 @@ void build_linv_schedule(const dct::Symbolic& S, dct::Schedule* sc,
   {
     Launch l{dct::kLinvInit, 0, int64_t(sc->tasks.size()), 0, 0};
     for (int s = 0; s < S.nsuper; ++s)
-      if (S.ns(s) > dct::kPanel)
+      if (S.ns(s) >= min_ns)
         for (int p = 0; p * dct::kPanel < S.ns(s); ++p) sc->tasks.push_back({s, p, 0, 0});
     l.count = int64_t(sc->tasks.size()) - l.first;
     if (l.count) sc->launches.push_back(l);
@@ -604,7 +627,7 @@ int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t whic
   dct::Schedule lv;
   std::vector<int64_t> loff;
   int64_t ltot = 0;
-  build_linv_schedule(h->sym, &lv, &loff, &ltot);
+  build_linv_schedule(h->sym, dtype, &lv, &loff, &ltot);
   const dct::Schedule& sc =
       which == 0 ? f : (which == 1 ? fw : (which == 2 ? bw : (which == 3 ? iv : lv)));
   const int64_t nt = int64_t(sc.tasks.size()), nl = int64_t(sc.launches.size());
@@ -688,7 +711,7 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
     P->d_dinv_off = d;
   }
   std::vector<int64_t> linv_off;
-  build_linv_schedule(S, &P->linv_sched, &linv_off, &P->linv_stride);
+  build_linv_schedule(S, dtype, &P->linv_sched, &linv_off, &P->linv_stride);
   {
     const int64_t* d = nullptr;
     if ((rc = upload(P, linv_off, &d))) return bail(rc);

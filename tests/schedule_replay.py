@@ -128,7 +128,6 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE):
         w = min(PANEL, ns - c0)
         dinv[(s, p)] = np.linalg.inv(np.tril(F[c0:c0 + w, c0:c0 + w]))
     elif kind == LINVINIT:
-        assert ns > PANEL
         c0 = p * PANEL
         w = min(PANEL, ns - c0)
         dinv[("linv", s)][c0:c0 + w, c0:c0 + w] = dinv[(s, p)]
@@ -158,8 +157,11 @@ def replay_factor(sym, S, vals, dtype=0):
     dinv = {}
     # supernode inverses and their scratch start as NaN: a read of an entry
     # that no earlier launch wrote poisons the result
+    # (float32 plans keep one for every supernode, float64 plans for those
+    # wider than one panel)
+    min_ns = 1 if dtype == 1 else PANEL + 1
     for s in range(S.nsuper):
-        if S.ns(s) > PANEL:
+        if S.ns(s) >= min_ns:
             dinv[("linv", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
             dinv[("ltmp", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
     utile = UTILE if dtype == 0 else 128
@@ -193,7 +195,7 @@ def replay_factor(sym, S, vals, dtype=0):
     assert len([k for k in dinv if k[0] not in ("linv", "ltmp")]) == npanels, \
         "a panel inverse was never stored"
     for s in range(S.nsuper):
-        if S.ns(s) > PANEL:
+        if S.ns(s) >= min_ns:
             X = dinv[("linv", s)]
             low = np.tril(np.ones_like(X, dtype=bool))
             assert not np.isnan(X[low]).any(), f"supernode {s}: inverse incomplete"
@@ -244,7 +246,6 @@ def _task_solve(S, kind, tk, fronts, A, B, dinv):
     elif kind in (FWDLINVTC, FWDBNDTC, BWDGEMMTC, BWDLINVTC):
         # tensor-core products: 128-row output tile t0, K range [p, t1),
         # accumulated (other tasks may add to the same rows)
-        assert ns > PANEL
         k0, k1, m0 = p, t1, t0 * TCTILE
         assert 0 <= k0 < k1
         if kind == FWDBNDTC:
