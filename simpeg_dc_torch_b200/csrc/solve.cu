@@ -443,11 +443,12 @@ __global__ void k_residual(DevSym S, const double* __restrict__ vals,
   const double* Bv = b + int64_t(bb) * bstride;
   float* R = r32 + int64_t(bb) * n * k;
   double rmax = 0.0, bmax = 0.0;
-  const int64_t total = int64_t(n) * k;
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int i = static_cast<int>(idx / k);
-    const int j = static_cast<int>(idx - int64_t(i) * k);
+  // n * k < 2^31 (checked at launch): 32-bit index arithmetic
+  const int total = n * k;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += gridDim.x * blockDim.x) {
+    const int i = idx / k;
+    const int j = idx - i * k;
     const int orow = S.perm[i];
     double acc = Bv[idx];
     bmax = fmax(bmax, fabs(acc));
@@ -618,6 +619,7 @@ cudaError_t launch_convert_any(const void* src, int src_dtype, int64_t sstride,
 cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
                             const double* x, int k, cudaStream_t st) {
   const int n = P->sym.n;
+  if (int64_t(n) * k >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
   dim3 g = grid1d(int64_t(n) * k, P->nbatch);
   k_residual<<<g, kThreads, 0, st>>>(
       P->ds, P->vals64, static_cast<int64_t>(P->sym.nnz_in), b, bstride, x, n, k,
