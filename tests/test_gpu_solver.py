@@ -158,3 +158,48 @@ def test_zero_pivot_is_reported_not_trapped(cuda):
 def test_cpu_device_is_refused():
     with pytest.raises(NotImplementedError):
         make_solver(torch.tensor([0, 1]), torch.tensor([0]), 1, 1, device="cpu")
+
+
+def _regularisation_hm(nx, ny, alpha_s, alpha_x, alpha_y, rng):
+    """H_m = alpha_s W_s + alpha_x Dx^T Wx Dx + alpha_y Dy^T Wy Dy on an
+    nx x ny cell grid (positive weights): SPD for alpha_s > 0, the shape of
+    the Gauss-Newton model Hessian the reference solves on the GPU."""
+    def diff(n):
+        return sp.diags([-np.ones(n - 1), np.ones(n - 1)], [0, 1], shape=(n - 1, n))
+    Dx = sp.kron(sp.eye(ny), diff(nx))
+    Dy = sp.kron(diff(ny), sp.eye(nx))
+    ws = sp.diags(rng.uniform(0.5, 2.0, nx * ny))
+    wx = sp.diags(rng.uniform(0.5, 2.0, Dx.shape[0]))
+    wy = sp.diags(rng.uniform(0.5, 2.0, Dy.shape[0]))
+    H = (alpha_s * ws + alpha_x * Dx.T @ wx @ Dx + alpha_y * Dy.T @ wy @ Dy).tocsr()
+    H.sort_indices()
+    return H
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_gauss_newton_hm_solve_call_site(cuda, k):
+    """The reference's TorchGaussNewton._hm_solve_gpu (dctorch/optimization.py:
+    727-761) plans once per pattern with make_solver(..., matrix_type='spd'),
+    refactorizes per step and accepts the solve when ||H X - rhs|| / ||rhs||
+    <= 1e-8.  The same sequence on this package's solver, two steps with
+    different values on one plan."""
+    rng = np.random.default_rng(11)
+    H = _regularisation_hm(90, 40, 1e-3, 1.0, 0.5, rng)
+    n = H.shape[0]
+    crow = torch.as_tensor(H.indptr, dtype=torch.int32, device=cuda)
+    col = torch.as_tensor(H.indices, dtype=torch.int32, device=cuda)
+    slv = make_solver(crow, col, n, k, device=cuda, dtype=torch.float64,
+                      matrix_type="spd")
+    for step in range(2):
+        Hs = H.copy()
+        Hs.data = Hs.data * (1.0 + 0.5 * step)
+        rhs = torch.as_tensor(rng.standard_normal((n, k)), device=cuda)
+        vals = torch.as_tensor(Hs.data, dtype=torch.float64, device=cuda)
+        slv.factorize(vals)
+        X = slv.solve(rhs.contiguous())
+        Ht = torch.sparse_csr_tensor(crow.long(), col.long(), vals, (n, n))
+        res = torch.linalg.norm(Ht @ X - rhs) / torch.linalg.norm(rhs)
+        assert float(res) <= 1e-8
+        ref = spla.spsolve(Hs.tocsc(), rhs.cpu().numpy())
+        assert rel(X.cpu(), torch.as_tensor(ref.reshape(n, k))) < 1e-10
+    assert slv.check() == 0.0
