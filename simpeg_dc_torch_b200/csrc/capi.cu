@@ -61,7 +61,7 @@ int ceil_div(int a, int b) { return (a + b - 1) / b; }
 // ---- schedules ------------------------------------------------------------
 // Algorithmic work of each launch (see dct::Schedule).  es = element size.
 void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
-                    int utile) {
+                    int utile, int bpan) {
   sc->flops.assign(sc->launches.size(), 0.0);
   sc->bytes.assign(sc->launches.size(), 0.0);
   sc->bytes_rhs.assign(sc->launches.size(), 0.0);
@@ -112,10 +112,12 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
             break;
           }
           const int base = c0 + w;
+          const dct::UpdateRange R = dct::update_range(t.p, ns, N, bpan);
+          const double kk = base - R.ka;
           const double ni = std::min(utile, N - (base + t.t0 * utile));
-          const double nj = std::min(utile, N - (base + t.t1 * utile));
-          f += 2 * ni * nj * w;
-          b += es * ((ni + nj) * w + 2 * ni * nj);
+          const double nj = std::min(utile, R.cend - (base + t.t1 * utile));
+          f += 2 * ni * nj * kk;
+          b += es * ((ni + nj) * kk + 2 * ni * nj);
           if (t.t0 == 0 && t.t1 == 0 && base < ns) {
             const double w2 = std::min(dct::kPanel, ns - base);
             f += 2.0 * w2 * w2 * w2 / 3.0;
@@ -197,8 +199,12 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
 // trailing-update tile: 64 for float64 (CUDA cores), 128 for float32
 // (tcgen05 tensor-core tiles, M = N = 128)
 int update_tile(int dtype) { return dtype == DCT_F64 ? dct::kUpdateTile : 128; }
+// panels per block of the trailing update (dct::update_range): float32
+// fronts defer the update of the columns beyond the block and apply it with
+// K = up to 4 panels; float64 fronts update after every panel
+int update_block(int dtype) { return dtype == DCT_F64 ? 1 : dct::kUpdateBlockPanels; }
 
-void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile,
+void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int bpan,
                            dct::Schedule* out) {
   auto& T = out->tasks;
   auto& L = out->launches;
@@ -263,9 +269,11 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile,
         int c0 = p * dct::kPanel;
         if (c0 >= ns) continue;
         int w = std::min(dct::kPanel, ns - c0);
-        int nt = ceil_div(N - c0 - w, utile);
-        for (int i = 0; i < nt; ++i)
-          for (int j = 0; j <= i; ++j) T.push_back({s, p, i, j});
+        const dct::UpdateRange R = dct::update_range(p, ns, N, bpan);
+        int nti = ceil_div(N - c0 - w, utile);
+        int ntj = ceil_div(R.cend - c0 - w, utile);
+        for (int i = 0; i < nti; ++i)
+          for (int j = 0; j <= i && j < ntj; ++j) T.push_back({s, p, i, j});
       }
       lu.count = int64_t(T.size()) - lu.first;
       L.push_back(lu);
@@ -619,7 +627,7 @@ int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t whic
     return fail(DCT_ERR_ARG, "bad arguments");
   dct::Schedule f, fw, bw, iv;
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(h->sym, small_max, update_tile(dtype), &f);
+  build_factor_schedule(h->sym, small_max, update_tile(dtype), update_block(dtype), &f);
   build_solve_schedules(h->sym, dtype, &fw, &bw);
   std::vector<int64_t> off;
   int64_t tot = 0;
@@ -701,7 +709,8 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
       (rc = upload(P, S.in_crow, &D.crow)) || (rc = upload(P, S.in_col, &D.col)))
     return bail(rc);
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(S, small_max, update_tile(dtype), &P->fact);
+  build_factor_schedule(S, small_max, update_tile(dtype), update_block(dtype), &P->fact);
+  P->update_bpan = update_block(dtype);
   build_solve_schedules(S, dtype, &P->fwd, &P->bwd);
   std::vector<int64_t> dinv_off;
   build_inverse_schedule(S, small_max, &P->inv, &dinv_off, &P->dinv_stride);
@@ -717,7 +726,8 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
     if ((rc = upload(P, linv_off, &d))) return bail(rc);
     P->d_linv_off = d;
   }
-  account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype));
+  account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype),
+                 update_block(dtype));
   account_solve(S, &P->fwd, double(esize(dtype)));
   account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||

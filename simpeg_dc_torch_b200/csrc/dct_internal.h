@@ -69,6 +69,31 @@ constexpr int kThreads = 256;
 constexpr int kRhsChunk = 64;   // right-hand sides per CTA in the solves
 constexpr int kRowGroup = 4;    // 64-row tiles per CTA in forward panel steps
 constexpr int kUpdateTile = 64;   // trailing-update tile (rows = cols)
+// float32 fronts group their panels in blocks of this many for the trailing
+// update (see update_range); float64 fronts update after every panel
+constexpr int kUpdateBlockPanels = 4;
+
+// Column ranges of the trailing update that follows panel p of a supernode
+// with ns columns (front order N) when the panels are grouped in blocks of
+// bpan (LAPACK-style blocked right-looking Cholesky with an inner panel
+// loop): the last panel of a block, or of the supernode, updates the whole
+// trailing block, columns [base, N), with all of the block's panels as K
+// (columns [ka, base)); any other panel updates only the remaining columns
+// of its own block, [base, cend), with its own kPanel columns.  base = the
+// first column after panel p.  bpan = 1 is the plain right-looking update.
+struct UpdateRange {
+  int ka, cend;
+};
+__host__ __device__ inline UpdateRange update_range(int p, int ns, int N, int bpan) {
+  const int npan = (ns + kPanel - 1) / kPanel;
+  const int blk = p / bpan;
+  const bool last = (p % bpan == bpan - 1) || (p == npan - 1);
+  UpdateRange r;
+  r.ka = (last ? blk * bpan : p) * kPanel;
+  const int bend = (blk + 1) * bpan * kPanel;
+  r.cend = last ? N : (bend < ns ? bend : ns);
+  return r;
+}
 
 struct Schedule {
   std::vector<PanelTask> tasks;    // host copy
@@ -137,6 +162,7 @@ struct dct_plan {
   int factored = 0;
   int64_t stamp = 0;
   int ir_iters = 2;                // refinement iterations of f32 plans
+  int update_bpan = 1;             // panels per trailing-update block
   dct::Profiler prof;
 };
 

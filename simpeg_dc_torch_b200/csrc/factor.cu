@@ -521,64 +521,44 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 }
 
 // ------------------------------------------------------------ tensor cores
-// float32 fronts: the 128 x 128 trailing-update tile F_ij -= L_i L_j^T on the
-// 5th-generation tensor cores (tcgen05.mma kind::tf32, accumulator in TMEM).
-// Each float32 operand x is split as x_hi = tf32(x), x_lo = tf32(x - x_hi),
-// and the product is x_hi y_hi + x_hi y_lo + x_lo y_hi (the 3xTF32 scheme of
-// Markidis et al., 2018, and Ootomo & Yokota, 2022), which restores float32
-// accuracy from TF32 products accumulated in float32.
+// float32 fronts: the trailing update F_ij -= L_i L_j^T of one 128 x 128 tile
+// on the 5th-generation tensor cores (tcgen05.mma kind::tf32, accumulator in
+// TMEM), with K = the columns [ka, base) given by update_range: one panel for
+// the narrow updates inside a block of panels, up to kUpdateBlockPanels
+// panels for the deferred update of the columns beyond the block, so that
+// the trailing block is read and written once per block instead of once per
+// panel.  Each float32 operand x is split as x_hi = tf32(x),
+// x_lo = tf32(x - x_hi), and the product is x_hi y_hi + x_hi y_lo + x_lo y_hi
+// (the 3xTF32 scheme of Markidis et al., 2018, and Ootomo & Yokota, 2022),
+// which restores float32 accuracy from TF32 products accumulated in float32.
 //
-// Shared-memory operands are K-major without swizzle: core matrices of
-// 8 rows x 16 bytes (4 values), element (m, k) at byte
-//   (m / 8) * SBO + (k / 4) * LBO + (m % 8) * 16 + (k % 4) * 4,
-// LBO = 128 (next 4 values of k), SBO = 2048 (next 8 rows; 64 values of k).
-// One MMA covers K = 8: its descriptors start 256 bytes further per step.
-// split the rows [r0, r0+nr) x columns [c0, c0+w) of front F (float) into the
-// hi/lo K-major operands at `hi`/`lo` (zero beyond nr rows and w columns).
-// Lane l of a warp handles row m_lo = l / 4 and column k_lo = l % 4 of one
-// 8 x 4 core matrix, so each warp stores one contiguous 128-byte block per
-// operand (no bank conflicts) and reads four 32-byte pieces of the front.
-__device__ __forceinline__ void load_split(const float* __restrict__ F, int N, int r0,
-                                           int nr, int c0, int w, unsigned char* hi,
-                                           unsigned char* lo) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int kWarps = kTcThreads / 32;
-  constexpr int kCores = (kTcM / 8) * (kPanel / 4);   // 16 x 16 core matrices
-  constexpr int kPer = kCores / kWarps;
-  const int m_lo = lane >> 2, k_lo = lane & 3;   // lane = m_lo * 4 + k_lo
-  // every load of this warp is issued before any shared store
-  float v[kPer];
-#pragma unroll
-  for (int u = 0; u < kPer; ++u) {
-    const int cm = warp + u * kWarps;
-    const int m = (cm % (kTcM / 8)) * 8 + m_lo, k = (cm / (kTcM / 8)) * 4 + k_lo;
-    v[u] = (m < nr && k < w) ? F[(r0 + m) + int64_t(c0 + k) * N] : 0.0f;
-  }
-#pragma unroll
-  for (int u = 0; u < kPer; ++u) {
-    const int cm = warp + u * kWarps;
-    tc_store_split(hi, lo, (cm % (kTcM / 8)) * kTcSBO + (cm / (kTcM / 8)) * kTcLBO + lane * 4,
-                   v[u]);
-  }
-}
+// K is staged 32 columns at a time through a two-stage shared-memory ring;
+// the next stage's operands are loaded into registers while the MMAs of the
+// current stage run.  Shared-memory operands are K-major without swizzle:
+// core matrices of 8 rows x 16 bytes (4 values), element (m, k) at byte
+//   (m / 8) * kUpSbo + (k / 4) * kUpLbo + (m % 8) * 16 + (k % 4) * 4.
+// Lane l of a warp handles row m % 8 = l / 4 and column k % 4 = l % 4 of one
+// core matrix, so each warp stores one contiguous 128-byte block per operand
+// (no bank conflicts) and reads four 32-byte pieces of the front.
+constexpr int kUpStK = 32;                                   // K per stage
+constexpr uint32_t kUpLbo = 128, kUpSbo = (kUpStK / 4) * kUpLbo;   // 1024
+constexpr int kUpOpBytes = (kTcM / 8) * kUpSbo;              // 128 x 32 floats
+constexpr int kUpStageBytes = 4 * kUpOpBytes;                // A hi/lo, B hi/lo
+constexpr int kUpPer = (kTcM / 8) * (kUpStK / 4) / (kTcThreads / 32);   // 8
 
-// task: s, p, t0 = i, t1 = j (i >= j) over 128-row tiles of the trailing
-// block after panel p, or t0 = -1: factor the diagonal block of panel p.
-// The CTA of tile (0, 0) factors the next panel's diagonal block afterwards.
+// task: s, p, t0 = i, t1 = j (i >= j) over 128-row / 128-column tiles of the
+// trailing block after panel p (columns up to update_range's cend), or
+// t0 = -1: factor the diagonal block of panel p.  The CTA of tile (0, 0)
+// factors the next panel's diagonal block afterwards.
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
                   int64_t front_stride, float* dinv, const int64_t* dinv_off,
-                  int64_t dinv_stride, int* status) {
+                  int64_t dinv_stride, int bpan, int* status) {
   // dynamic shared memory is 16-byte aligned, all the descriptors need;
   // addressing it directly keeps the accesses in the shared state space
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned char* base_ptr = smem_raw;
-  unsigned char* Ahi = base_ptr;
-  unsigned char* Alo = Ahi + kTcOperandBytes;
-  unsigned char* Bhi = Alo + kTcOperandBytes;
-  unsigned char* Blo = Bhi + kTcOperandBytes;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + kTcOperandBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * kUpStageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
 
   const PanelTask tk = tasks[blockIdx.x];
   const int b = blockIdx.y;
@@ -591,54 +571,123 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   float* F = fronts + int64_t(b) * front_stride + S.front_off[s];
   float* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  float* sm = reinterpret_cast<float*>(base_ptr);
+  float* sm = reinterpret_cast<float*>(smem_raw);
   if (tk.t0 < 0) {
     factor_diag<float, kTcThreads>(F, N, c0, w, sm, Dv + int64_t(tk.p) * kPanel * kPanel, status, s,
                                     b);
     return;
   }
+  const UpdateRange R = update_range(tk.p, ns, N, bpan);
   const int ri = base + tk.t0 * kTcM, rj = base + tk.t1 * kTcN;
-  const int ni = min(kTcM, N - ri), nj = min(kTcN, N - rj);
+  const int ni = min(kTcM, N - ri), nj = min(kTcN, R.cend - rj);
+  const int np = (nj + 15) & ~15;   // MMA N: a multiple of 16
+  const int nst = (base - R.ka + kUpStK - 1) / kUpStK;
 
   if (warp == 0) tmem_alloc(tmem_slot, kTcN);
-  if (tid == 0) mbar_init(mbar);
-  load_split(F, N, ri, ni, c0, w, Ahi, Alo);
-  load_split(F, N, rj, nj, c0, w, Bhi, Blo);
-  tc_publish_smem();
+  if (tid == 0) {
+    mbar_init(&mbar[0]);
+    mbar_init(&mbar[1]);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  if (tid == 0)
-    umma_3xtf32(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo),
-                (w + 7) / 8, umma_idesc_tf32(kTcM, kTcN), 0, mbar);
-  const bool done = tc_wait(mbar, 0, status, DCT_ERR_DEVICE_TIMEOUT, s, b);
-  if (done) {
+  const uint32_t idesc = umma_idesc_tf32(kTcM, np);
+  // slot u of this thread: core matrix cm = warp + 16 u, rows
+  // m = 8 (cm % 16) + lane / 4, columns kl = 4 (cm / 16) + lane % 4
+  const int m_lo = lane >> 2, k_lo = lane & 3;
+  float va[kUpPer], vb[kUpPer];
+  // the panel columns [ka, base) are read-only in this launch (all writes
+  // go to columns >= base), so the read-only path is safe
+  auto load_stage = [&](int st) {
+    const int kb = R.ka + st * kUpStK;
+    const int kw = min(kUpStK, base - kb);
+#pragma unroll
+    for (int u = 0; u < kUpPer; ++u) {
+      const int cm = warp + u * (kTcThreads / 32);
+      const int m = (cm % (kTcM / 8)) * 8 + m_lo, kl = (cm / (kTcM / 8)) * 4 + k_lo;
+      const int64_t col = int64_t(kb + kl) * N;
+      va[u] = (m < ni && kl < kw) ? __ldg(F + (ri + m) + col) : 0.0f;
+      vb[u] = (m < nj && kl < kw) ? __ldg(F + (rj + m) + col) : 0.0f;
+    }
+  };
+  bool ok = true;
+  load_stage(0);
+  for (int st = 0; st < nst; ++st) {
+    const int buf = st & 1;
+    // the ring slot is free once the MMAs of stage st - 2 have completed
+    if (st >= 2) {
+      ok = tc_wait(&mbar[buf], uint32_t((st - 2) >> 1) & 1u, status,
+                   DCT_ERR_DEVICE_TIMEOUT, s, b);
+      if (!ok) break;
+    }
+    unsigned char* Ahi = smem_raw + buf * kUpStageBytes;
+    unsigned char* Alo = Ahi + kUpOpBytes;
+    unsigned char* Bhi = Alo + kUpOpBytes;
+    unsigned char* Blo = Bhi + kUpOpBytes;
+    const int kw = min(kUpStK, base - (R.ka + st * kUpStK));
+#pragma unroll
+    for (int u = 0; u < kUpPer; ++u) {
+      const int cm = warp + u * (kTcThreads / 32);
+      const uint32_t off =
+          uint32_t(cm % (kTcM / 8)) * kUpSbo + uint32_t(cm / (kTcM / 8)) * kUpLbo + lane * 4;
+      tc_store_split(Ahi, Alo, off, va[u]);
+      tc_store_split(Bhi, Blo, off, vb[u]);
+    }
+    if (st + 1 < nst) load_stage(st + 1);
+    tc_publish_smem();
+    if (tid == 0) {
+      const uint32_t ah = smem_u32(Ahi), al = smem_u32(Alo);
+      const uint32_t bh = smem_u32(Bhi), bl = smem_u32(Blo);
+      for (int kk = 0; kk < (kw + 7) / 8; ++kk) {
+        const uint32_t ko = uint32_t(kk) * 2 * kUpLbo;
+        const uint64_t dah = umma_desc(ah + ko, kUpLbo, kUpSbo);
+        const uint64_t dal = umma_desc(al + ko, kUpLbo, kUpSbo);
+        const uint64_t dbh = umma_desc(bh + ko, kUpLbo, kUpSbo);
+        const uint64_t dbl = umma_desc(bl + ko, kUpLbo, kUpSbo);
+        umma_tf32(tmem, dah, dbh, idesc, (st > 0 || kk > 0) ? 1u : 0u);
+        umma_tf32(tmem, dah, dbl, idesc, 1u);
+        umma_tf32(tmem, dal, dbh, idesc, 1u);
+      }
+      umma_commit(&mbar[buf]);
+    }
+  }
+  // the last commit tracks every MMA issued before it
+  if (ok)
+    ok = tc_wait(&mbar[(nst - 1) & 1], uint32_t((nst - 1) >> 1) & 1u, status,
+                 DCT_ERR_DEVICE_TIMEOUT, s, b);
+  if (ok) {
     // warp w reads TMEM lanes (tile rows) 32(w%4) .. +31, columns 32(w/4) .. +31
     const int row = (warp & 3) * 32 + lane;
     const int cb = (warp >> 2) * 32;
-    uint32_t v[32];
-    tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
-    if (row < ni) {
-      float* dst = F + (ri + row) + int64_t(rj + cb) * N;
-      float cur[32];
+    if (cb < np) {
+      uint32_t v[32];
+      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+      if (row < ni) {
+        float* dst = F + (ri + row) + int64_t(rj + cb) * N;
+        float cur[32];
 #pragma unroll
-      for (int c = 0; c < 32; ++c) cur[c] = (cb + c < nj) ? dst[int64_t(c) * N] : 0.0f;
+        for (int c = 0; c < 32; ++c) cur[c] = (cb + c < nj) ? dst[int64_t(c) * N] : 0.0f;
 #pragma unroll
-      for (int c = 0; c < 32; ++c)
-        if (cb + c < nj) dst[int64_t(c) * N] = cur[c] - __uint_as_float(v[c]);
+        for (int c = 0; c < 32; ++c)
+          if (cb + c < nj) dst[int64_t(c) * N] = cur[c] - __uint_as_float(v[c]);
+      }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, kTcN);
-  if (done && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
+  if (ok && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
     __syncthreads();   // this CTA's updates of the block are complete
     factor_diag<float, kTcThreads>(F, N, base, min(kPanel, ns - base), sm,
                 Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
   }
 }
 
-constexpr size_t kTcSmem = 4 * size_t(kTcOperandBytes) + 64;
-static_assert(4 * size_t(kTcOperandBytes) >= sizeof(float) * kDiagSmemElems,
+constexpr size_t kTcSmem = 2 * size_t(kUpStageBytes) + 64;
+static_assert(2 * size_t(kUpStageBytes) >= sizeof(float) * kDiagSmemElems,
               "tensor-core update smem must also hold factor_diag's workspace");
+static_assert(kUpSbo % 16 == 0 && kUpOpBytes % 16 == 0, "descriptor alignment");
 
 // task: s, p.  D_p^{-1} of the factored diagonal block of panel p of a small
 // front, written column-major (ld w) at dinv + dinv_off[s] + p*64*64.
@@ -890,7 +939,7 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
           k_large_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(
               P->ds, t, reinterpret_cast<float*>(fronts), P->front_stride,
               static_cast<float*>(P->dinv), P->d_dinv_off, P->dinv_stride,
-              P->status);
+              P->update_bpan, P->status);
         } else {
           k_large_update<T><<<grid, kThreads, update_smem, st>>>(
               P->ds, t, fronts, P->front_stride, static_cast<T*>(P->dinv),

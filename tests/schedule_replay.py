@@ -59,7 +59,20 @@ def _factor_diag(S, F, s, c0, w, dinv):
     dinv[(s, c0 // PANEL)] = np.linalg.inv(L)
 
 
-def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE):
+def update_range(p, ns, N, bpan):
+    """K columns [ka, base) and last column cend of the trailing update after
+    panel p when panels are grouped in blocks of bpan (libdct's
+    dct::update_range): a block's last panel updates everything beyond the
+    block with all of its panels, the others only the rest of their block."""
+    npan = -(-ns // PANEL)
+    blk = p // bpan
+    last = p % bpan == bpan - 1 or p == npan - 1
+    ka = (blk * bpan if last else p) * PANEL
+    cend = N if last else min((blk + 1) * bpan * PANEL, ns)
+    return ka, cend
+
+
+def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE, bpan=1):
     s, p, t0, t1 = (int(v) for v in tk)
     N = int(S.front_n[s])
     ns = S.ns(s)
@@ -116,11 +129,12 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE):
         if t0 < 0:
             _factor_diag(S, F, s, c0, w, dinv)
             return
+        ka, cend = update_range(p, ns, N, bpan)
         ri, rj = base + t0 * utile, base + t1 * utile
-        assert ri < N and rj < N and t0 >= t1
-        ni, nj = min(utile, N - ri), min(utile, N - rj)
-        F[ri:ri + ni, rj:rj + nj] -= (F[ri:ri + ni, c0:c0 + w]
-                                      @ F[rj:rj + nj, c0:c0 + w].T)
+        assert ri < N and rj < cend and t0 >= t1
+        ni, nj = min(utile, N - ri), min(utile, cend - rj)
+        F[ri:ri + ni, rj:rj + nj] -= (F[ri:ri + ni, ka:base]
+                                      @ F[rj:rj + nj, ka:base].T)
         if t0 == 0 and t1 == 0 and base < ns:
             _factor_diag(S, F, s, base, min(PANEL, ns - base), dinv)
     elif kind == PINV:
@@ -165,6 +179,7 @@ def replay_factor(sym, S, vals, dtype=0):
             dinv[("linv", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
             dinv[("ltmp", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
     utile = UTILE if dtype == 0 else 128
+    bpan = 1 if dtype == 0 else 4
 
     def snapshot(d):
         return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
@@ -175,11 +190,11 @@ def replay_factor(sym, S, vals, dtype=0):
             chunk = tasks[first:first + count]
             snap, dsnap = fronts.copy(), snapshot(dinv)
             for tk in chunk:
-                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
+                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile, bpan)
             fwd_result, fwd_dinv = fronts.copy(), snapshot(dinv)
             fronts[:], dinv = snap, dsnap
             for tk in chunk[::-1]:
-                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile)
+                _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile, bpan)
             scale = max(1.0, np.abs(fwd_result).max())
             assert np.abs(fronts - fwd_result).max() <= 1e-9 * scale, \
                 f"launch kind {kind} level {lv}: result depends on task order"

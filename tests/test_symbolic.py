@@ -83,6 +83,26 @@ def test_replay_reference_laplacian_without_coordinates():
     assert err < 1e-12
 
 
+@pytest.mark.parametrize("dtype", [0, 1])
+def test_replay_wide_supernode_blocked_update(dtype):
+    """A dense 330 x 330 block coupled to a 2-D grid: one supernode of six
+    panels, i.e. a full block of four panels and a partial one, so that the
+    float32 schedule's deferred K = 256 updates (and the narrow updates
+    inside each block) are replayed."""
+    rng = np.random.default_rng(3)
+    G = rng.standard_normal((330, 330))
+    D = sp.csr_matrix(G @ G.T / 330 + 4 * np.eye(330))
+    L = laplacian(12)
+    C = sp.random(L.shape[0], 330, density=0.02, random_state=4) * 0.05
+    A = sp.bmat([[L + 2 * sp.eye(L.shape[0]), C], [C.T, D]]).tocsr()
+    A = ((A + A.T) * 0.5).tocsr()
+    A.sort_indices()
+    rhs = rng.standard_normal((A.shape[0], 3))
+    err, info = _check(A, None, 32, rhs, dtype)
+    assert err < 1e-11
+    assert info["max_ns"] > 4 * 64
+
+
 def test_disconnected_pattern():
     A = sp.block_diag([laplacian(6), laplacian(5), sp.eye(3) * 2.0]).tocsr()
     A.sort_indices()
