@@ -134,11 +134,24 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
 }
 
 // Tensor-core substitution tasks: one 128-row output tile t and a K range
-// [k0, k1) per task (PanelTask {s, k0, t, k1}); ranges longer than kTcSplitK
-// are split so that the top levels of the tree, which hold few supernodes,
-// still fill the GPU.  Within a launch the longest tasks come first.
+// [k0, k1) per task (PanelTask {s, k0, t, k1}).  K ranges are split into
+// pieces of at most kTcSplitK columns; a launch with fewer than
+// kTcTargetCtas tasks halves the piece (down to kTcSplitMin) so that the top
+// levels of the tree, which hold few supernodes, still fill the GPU.  Within
+// a launch the longest tasks come first.
 constexpr int kTcTile = 128;
-constexpr int kTcSplitK = 512;
+#ifndef DCT_TC_SPLITK
+#define DCT_TC_SPLITK 512
+#endif
+#ifndef DCT_TC_TARGET_CTAS
+#define DCT_TC_TARGET_CTAS 592   // four waves of 148 SMs
+#endif
+#ifndef DCT_TC_SPLIT_MIN
+#define DCT_TC_SPLIT_MIN 128
+#endif
+constexpr int kTcSplitK = DCT_TC_SPLITK;
+constexpr int kTcTargetCtas = DCT_TC_TARGET_CTAS;
+constexpr int kTcSplitMin = DCT_TC_SPLIT_MIN;
 
 void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
   sc->flops.assign(sc->launches.size(), 0.0);
@@ -287,8 +300,8 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int
 // (kFwdLinv / kBwdLinv, 64-row tiles) and exchange with their boundary rows
 // once (kFwdBnd[Tc] after, kBwdGemm before).  A pass is a few launches per
 // level, independent of the supernodes' widths.
-void push_split(std::vector<PanelTask>& T, int s, int t, int k0, int k1) {
-  for (int a = k0; a < k1; a += kTcSplitK) T.push_back({s, a, t, std::min(k1, a + kTcSplitK)});
+void push_split(std::vector<PanelTask>& T, int s, int t, int k0, int k1, int split) {
+  for (int a = k0; a < k1; a += split) T.push_back({s, a, t, std::min(k1, a + split)});
 }
 
 void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
@@ -314,9 +327,16 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
     small_tc = all > 0 && big >= 0.5 * all;
   }
   auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel && !small_tc; };
+  int split = kTcSplitK;   // K piece of the tensor-core tasks being filled
+  std::vector<PanelTask> tmp;
   auto add = [&](dct::Schedule* sc, int kind, int lv, auto&& fill) {
     Launch l{kind, lv, int64_t(sc->tasks.size()), 0, 0};
-    fill(sc->tasks);
+    for (split = kTcSplitK;; split /= 2) {
+      tmp.clear();
+      fill(tmp);
+      if (!tc || int64_t(tmp.size()) >= kTcTargetCtas || split / 2 < kTcSplitMin) break;
+    }
+    sc->tasks.insert(sc->tasks.end(), tmp.begin(), tmp.end());
     l.count = int64_t(sc->tasks.size()) - l.first;
     if (tc && l.count)
       std::stable_sort(sc->tasks.begin() + l.first, sc->tasks.end(),
@@ -337,7 +357,7 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
         if (is_small(s)) continue;
         if (tc) {
           for (int t = 0; t * kTcTile < ns; ++t)
-            push_split(T, s, t, 0, std::min(ns, (t + 1) * kTcTile));
+            push_split(T, s, t, 0, std::min(ns, (t + 1) * kTcTile), split);
         } else {
           for (int t = 0; t * dct::kPanel < ns; ++t) T.push_back({s, 0, t, 0});
         }
@@ -348,7 +368,7 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
         const int s = S.level_sn[q];
         if (is_small(s)) continue;
         if (tc) {
-          for (int t = 0; t < ceil_div(S.nb(s), kTcTile); ++t) push_split(T, s, t, 0, S.ns(s));
+          for (int t = 0; t < ceil_div(S.nb(s), kTcTile); ++t) push_split(T, s, t, 0, S.ns(s), split);
         } else {
           for (int t = 0; t < ceil_div(S.nb(s), dct::kPanel); ++t) T.push_back({s, 0, t, 0});
         }
@@ -366,7 +386,7 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
         const int s = S.level_sn[q], ns = S.ns(s);
         if (is_small(s) || S.nb(s) == 0) continue;
         if (tc) {
-          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, 0, S.nb(s));
+          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, 0, S.nb(s), split);
         } else {
           for (int p = 0; p * dct::kPanel < ns; ++p) T.push_back({s, p, 0, 0});
         }
@@ -377,7 +397,7 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
         const int s = S.level_sn[q], ns = S.ns(s);
         if (is_small(s)) continue;
         if (tc) {
-          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, t * kTcTile, ns);
+          for (int t = 0; t * kTcTile < ns; ++t) push_split(T, s, t, t * kTcTile, ns, split);
         } else {
           for (int t = 0; t * dct::kPanel < ns; ++t) T.push_back({s, 0, t, 0});
         }

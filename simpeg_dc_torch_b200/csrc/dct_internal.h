@@ -36,7 +36,9 @@ struct Launch {
   int level;
   int64_t first;
   int64_t count;
-  int arg;         // small fronts: largest front order of the launch
+  int arg;         // small fronts: largest front order of the launch;
+                   // panel steps: the panel; supernode inverses: the block
+                   // width
 };
 
 enum LaunchKind : int {

@@ -15,8 +15,11 @@
 // before the pass that writes them (see solve.cu).  tcgen05.mma kind::tf32
 // with the 3xTF32 split (hi*hi + hi*lo + lo*hi: Markidis et al. 2018; Ootomo
 // and Yokota 2022) accumulates in TMEM; operands are staged through registers
-// (the split needs them there) into a two-stage shared-memory ring so that
-// the loads of stage i+1 overlap the MMAs of stage i.
+// (the split needs them there) into shared memory; the loads of stage i+1
+// are issued before the MMAs of stage i.  The kernel runs 256 threads with
+// one 106 KB stage so that two CTAs share an SM and overlap each other's
+// load latency and fixed per-task cost; measured on B200 this beats one CTA
+// of 512 threads with a two-stage ring at every level of the tree.
 #include <cuda_runtime.h>
 
 #include "dct_internal.h"
@@ -27,7 +30,6 @@ namespace {
 
 constexpr int kStK = 32;                     // K per pipeline stage
 constexpr int kStN = 256;                    // right-hand sides per CTA
-constexpr int kWarps = kTcThreads / 32;
 // A operand (128 x 32): K-adjacent core matrices 160 B apart, so that the
 // transposed loaders (2 rows x 16 K per warp instruction) and the natural
 // ones (8 rows x 4 K) both store to 32 distinct banks.
@@ -39,20 +41,24 @@ constexpr int kABytes = (kTcM / 8) * kASbo;                    // 19968
 constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo + 16;   // 1040
 constexpr int kBBytes = (kStN / 8) * kBSbo;                         // 33280
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
-constexpr size_t kSolveTcSmem = 2 * size_t(kStageBytes) + 64;
-static_assert(kSolveTcSmem <= 232448, "shared memory of the tensor-core solve");
+constexpr int kNT = 256;       // threads per CTA
+constexpr int kRing = 1;       // shared-memory stages
+constexpr size_t kSolveTcSmem = kRing * size_t(kStageBytes) + 64;
+static_assert(2 * (kSolveTcSmem + 1024) <= 233472, "two CTAs per SM");
 static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
                   kBBytes % 16 == 0, "descriptor alignment");
 
 enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
 
 template <int MODE>
-__global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) {
+__global__ void __launch_bounds__(kNT, 2) k_solve_tc(SolveArgs<float> g) {
   constexpr bool kTrans = MODE == kModeBwdGemm || MODE == kModeBwdLinv;
   constexpr bool kInv = MODE == kModeFwdLinv || MODE == kModeBwdLinv;
+  constexpr int kWarps = kNT / 32;
+  static_assert(kWarps % 4 == 0, "whole warpgroups: TMEM lane quarters");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + 2 * kStageBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kRing * kStageBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kRing);
   const PanelTask tk = g.tasks[blockIdx.x];
   const int b = blockIdx.y / g.nchunk;
   const int j0 = (blockIdx.y % g.nchunk) * kStN;
@@ -86,10 +92,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) tmem_alloc(tmem_slot, kStN);
-  if (tid == 0) {
-    mbar_init(&mbar[0]);
-    mbar_init(&mbar[1]);
-  }
+  if (tid == 0)
+    for (int i = 0; i < kRing; ++i) mbar_init(&mbar[i]);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -98,8 +102,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   const int nst = (k1 - k0 + kStK - 1) / kStK;
   bool ok = true;
   // operand registers: stage st + 1 is loaded while the MMAs of stage st run
-  constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 8
-  constexpr int kPerB = kStN * kStK / 4 / kTcThreads;        // 4 float4
+  constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 16
+  constexpr int kPerB = kStN * kStK / 4 / kNT;                // 8 float4
   float va[kPerA];
   float4 vb[kPerB];
   const bool vec4 = (g.k & 3) == 0;   // 16-byte aligned rows
@@ -163,10 +167,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   };
   if (nst > 0) load_stage(0);
   for (int st = 0; st < nst; ++st) {
-    const int buf = st & 1;
-    // the ring slot is free once the MMAs of stage st - 2 have completed
-    if (st >= 2) {
-      ok = tc_wait(&mbar[buf], uint32_t((st - 2) >> 1) & 1u, g.status,
+    const int buf = st % kRing;
+    // the ring slot is free once the MMAs of stage st - kRing have completed
+    if (st >= kRing) {
+      ok = tc_wait(&mbar[buf], uint32_t((st - kRing) / kRing) & 1u, g.status,
                    DCT_ERR_DEVICE_TIMEOUT, s, b);
       if (!ok) break;
     }
@@ -219,7 +223,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
   }
   // the last commit tracks every MMA issued before it
   if (ok && nst > 0)
-    ok = tc_wait(&mbar[(nst - 1) & 1], uint32_t((nst - 1) >> 1) & 1u, g.status,
+    ok = tc_wait(&mbar[(nst - 1) % kRing], uint32_t((nst - 1) / kRing) & 1u, g.status,
                  DCT_ERR_DEVICE_TIMEOUT, s, b);
   if (ok && nst > 0) {
     const int m = (warp & 3) * 32 + lane;
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_solve_tc(SolveArgs<float> g) 
     }
     const float sgn = kInv ? 1.0f : -1.0f;
     const bool vec = (g.k & 3) == 0;   // 16-byte aligned rows
-    for (int cb = (warp >> 2) * 32; cb < np; cb += 4 * 32) {
+    for (int cb = (warp >> 2) * 32; cb < np; cb += (kWarps / 4) * 32) {
       uint32_t v[32];
       tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
       if (dst != nullptr) {
@@ -276,10 +280,10 @@ cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g0, int64_t count,
                                        static_cast<int>(kSolveTcSmem));
   if (e != cudaSuccess) return e;
   switch (kind) {
-    case kFwdLinvTc: k_solve_tc<kModeFwdLinv><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
-    case kFwdBndTc: k_solve_tc<kModeFwdBnd><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
-    case kBwdGemmTc: k_solve_tc<kModeBwdGemm><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
-    default: k_solve_tc<kModeBwdLinv><<<grid, kTcThreads, kSolveTcSmem, st>>>(g); break;
+    case kFwdLinvTc: k_solve_tc<kModeFwdLinv><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
+    case kFwdBndTc: k_solve_tc<kModeFwdBnd><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
+    case kBwdGemmTc: k_solve_tc<kModeBwdGemm><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
+    default: k_solve_tc<kModeBwdLinv><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
   }
   return cudaGetLastError();
 }
