@@ -73,7 +73,10 @@ constexpr int kRowGroup = 4;    // 64-row tiles per CTA in forward panel steps
 constexpr int kUpdateTile = 64;   // trailing-update tile (rows = cols)
 // float32 fronts group their panels in blocks of this many for the trailing
 // update (see update_range); float64 fronts update after every panel
-constexpr int kUpdateBlockPanels = 4;
+#ifndef DCT_UPDATE_BLOCK_PANELS
+#define DCT_UPDATE_BLOCK_PANELS 4
+#endif
+constexpr int kUpdateBlockPanels = DCT_UPDATE_BLOCK_PANELS;
 
 // Column ranges of the trailing update that follows panel p of a supernode
 // with ns columns (front order N) when the panels are grouped in blocks of
@@ -191,8 +194,6 @@ struct SolveArgs {
   const int64_t* linv_off;
   int64_t linv_stride;
 };
-// right-hand sides per CTA of the tensor-core substitution kernels
-constexpr int kSolveTcRhs = 256;
 // one launch of a tensor-core substitution kind (kFwdLinvTc .. kBwdLinvTc)
 cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g, int64_t count,
                             int nbatch, cudaStream_t st);

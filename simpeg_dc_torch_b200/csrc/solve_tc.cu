@@ -29,7 +29,13 @@ namespace dct {
 namespace {
 
 constexpr int kStK = 32;                     // K per pipeline stage
-constexpr int kStN = 256;                    // right-hand sides per CTA
+#ifndef DCT_TC_RHS
+#define DCT_TC_RHS 256
+#endif
+#ifndef DCT_TC_CTAS_PER_SM
+#define DCT_TC_CTAS_PER_SM 2
+#endif
+constexpr int kStN = DCT_TC_RHS;             // right-hand sides per CTA
 // A operand (128 x 32): K-adjacent core matrices 160 B apart, so that the
 // transposed loaders (2 rows x 16 K per warp instruction) and the natural
 // ones (8 rows x 4 K) both store to 32 distinct banks.
@@ -44,14 +50,15 @@ constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
 constexpr int kNT = 256;       // threads per CTA
 constexpr int kRing = 1;       // shared-memory stages
 constexpr size_t kSolveTcSmem = kRing * size_t(kStageBytes) + 64;
-static_assert(2 * (kSolveTcSmem + 1024) <= 233472, "two CTAs per SM");
+constexpr int kCtasPerSm = DCT_TC_CTAS_PER_SM;
+static_assert(kCtasPerSm * (kSolveTcSmem + 1024) <= 233472, "CTAs per SM");
 static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
                   kBBytes % 16 == 0, "descriptor alignment");
 
 enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
 
 template <int MODE>
-__global__ void __launch_bounds__(kNT, 2) k_solve_tc(SolveArgs<float> g) {
+__global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g) {
   constexpr bool kTrans = MODE == kModeBwdGemm || MODE == kModeBwdLinv;
   constexpr bool kInv = MODE == kModeFwdLinv || MODE == kModeBwdLinv;
   constexpr int kWarps = kNT / 32;
@@ -103,16 +110,17 @@ __global__ void __launch_bounds__(kNT, 2) k_solve_tc(SolveArgs<float> g) {
   bool ok = true;
   // operand registers: stage st + 1 is loaded while the MMAs of stage st run
   constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 16
-  constexpr int kPerB = kStN * kStK / 4 / kNT;                // 8 float4
+  constexpr int kPerB = kStN * kStK / 4 / kNT;                // 8 float4 (256 columns)
   float va[kPerA];
   float4 vb[kPerB];
   const bool vec4 = (g.k & 3) == 0;   // 16-byte aligned rows
-  // quad u of this thread: rows kl = 4 (warp-chunk) + lane % 4, quads
-  // n = 4 (8 (chunk) + lane / 4); 64 chunks of 4 rows x 32 columns
+  // quad u of this thread: rows kl = 4 (chunk / kNc) + lane % 4, quads
+  // n = 4 (8 (chunk % kNc) + lane / 4): chunks of 4 rows x 32 columns
+  constexpr int kNc = kStN / 32;
   auto b_coord = [&](int u, int& n, int& kl) {
-    const int c = warp + u * kWarps;           // 0 .. 63
-    kl = (c / 8) * 4 + (lane & 3);
-    n = ((c % 8) * 8 + (lane >> 2)) * 4;
+    const int c = warp + u * kWarps;           // 0 .. 8 kNc - 1
+    kl = (c / kNc) * 4 + (lane & 3);
+    n = ((c % kNc) * 8 + (lane >> 2)) * 4;
   };
   // element (m, kl) of A handled in slot u (fixed over the stages)
   auto a_coord = [&](int u, int& m, int& kl) {
@@ -264,7 +272,6 @@ __global__ void __launch_bounds__(kNT, 2) k_solve_tc(SolveArgs<float> g) {
 
 cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g0, int64_t count,
                             int nbatch, cudaStream_t st) {
-  static_assert(kStN == kSolveTcRhs, "right-hand sides per tensor-core CTA");
   SolveArgs<float> g = g0;
   g.nchunk = (g.k + kStN - 1) / kStN;
   dim3 grid(static_cast<unsigned>(count), static_cast<unsigned>(nbatch * g.nchunk));
