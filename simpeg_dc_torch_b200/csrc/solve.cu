@@ -430,8 +430,15 @@ __global__ void k_convert(const TI* __restrict__ src, int64_t sstride, int64_t c
 }
 
 // ------------------------------------------------------------ refinement
+// right-hand sides per thread of the refinement residual (1, 2 or 4)
+#ifndef DCT_RESIDUAL_RHS
+#define DCT_RESIDUAL_RHS 4
+#endif
+constexpr int kResidualRhs = DCT_RESIDUAL_RHS;
+
 // r = b - A x in float64 (permuted order), stored as float into the f32 work
 // buffer, with max|r| and max|b| folded into the plan's residual words.
+
 __global__ void k_residual(DevSym S, const double* __restrict__ vals,
                            int64_t vals_stride, const double* __restrict__ b,
                            int64_t bstride, const double* __restrict__ x, int n,
@@ -461,6 +468,69 @@ __global__ void k_residual(DevSym S, const double* __restrict__ vals,
   for (int o = 16; o > 0; o >>= 1) {
     rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
     bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&maxbits[0], __double_as_longlong(rmax));
+    atomicMax(&maxbits[1], __double_as_longlong(bmax));
+  }
+}
+
+// The same with RJ = 2 or 4 consecutive right-hand sides per thread (k a
+// multiple of RJ, rows 16-byte aligned): the row's pattern, permutation and
+// values are read once for RJ outputs, and x, b and r move as 16-byte vectors.
+template <int RJ>
+__global__ void k_residual_vec(DevSym S, const double* __restrict__ vals,
+                               int64_t vals_stride, const double* __restrict__ b,
+                               int64_t bstride, const double* __restrict__ x, int n,
+                               int k, float* __restrict__ r32,
+                               unsigned long long* __restrict__ maxbits) {
+  static_assert(RJ == 2 || RJ == 4, "two or four right-hand sides per thread");
+  const int bb = blockIdx.y;
+  const double* V = vals + int64_t(bb) * vals_stride;
+  const double* X = x + int64_t(bb) * n * k;
+  const double* Bv = b + int64_t(bb) * bstride;
+  float* R = r32 + int64_t(bb) * n * k;
+  double rmax = 0.0, bmax = 0.0;
+  const int kq = k / RJ;
+  // n * k < 2^31 (checked at launch): 32-bit index arithmetic
+  const int total = n * kq;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += gridDim.x * blockDim.x) {
+    const int i = idx / kq;
+    const int o = i * k + (idx - i * kq) * RJ;   // element (i, j)
+    const int orow = S.perm[i];
+    double acc[RJ];
+#pragma unroll
+    for (int h = 0; h < RJ; h += 2) {
+      const double2 v = *reinterpret_cast<const double2*>(Bv + o + h);
+      acc[h] = v.x;
+      acc[h + 1] = v.y;
+    }
+#pragma unroll
+    for (int h = 0; h < RJ; ++h) bmax = fmax(bmax, fabs(acc[h]));
+    const int j = o - i * k;
+    for (int e = S.crow[orow]; e < S.crow[orow + 1]; ++e) {
+      const double a = V[e];
+      const double* xr = X + S.iperm[S.col[e]] * k + j;
+#pragma unroll
+      for (int h = 0; h < RJ; h += 2) {
+        const double2 v = *reinterpret_cast<const double2*>(xr + h);
+        acc[h] -= a * v.x;
+        acc[h + 1] -= a * v.y;
+      }
+    }
+    if constexpr (RJ == 2) {
+      *reinterpret_cast<float2*>(R + o) = make_float2(float(acc[0]), float(acc[1]));
+    } else {
+      *reinterpret_cast<float4*>(R + o) =
+          make_float4(float(acc[0]), float(acc[1]), float(acc[2]), float(acc[3]));
+    }
+#pragma unroll
+    for (int h = 0; h < RJ; ++h) rmax = fmax(rmax, fabs(acc[h]));
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
+    bmax = fmax(bmax, __shfl_xor_sync(0xffffffffu, bmax, off));
   }
   if ((threadIdx.x & 31) == 0) {
     atomicMax(&maxbits[0], __double_as_longlong(rmax));
@@ -620,10 +690,26 @@ cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
                             const double* x, int k, cudaStream_t st) {
   const int n = P->sym.n;
   if (int64_t(n) * k >= (int64_t(1) << 31)) return cudaErrorInvalidValue;
-  dim3 g = grid1d(int64_t(n) * k, P->nbatch);
-  k_residual<<<g, kThreads, 0, st>>>(
-      P->ds, P->vals64, static_cast<int64_t>(P->sym.nnz_in), b, bstride, x, n, k,
-      static_cast<float*>(P->bufA), P->resid_bits);
+  const int64_t nnz = static_cast<int64_t>(P->sym.nnz_in);
+  float* r = static_cast<float*>(P->bufA);
+  // vector rows: k and the batch stride a multiple of kResidualRhs, 16-byte
+  // aligned b and x (buffer A comes from cudaMalloc)
+  const bool vec = kResidualRhs > 1 && k % kResidualRhs == 0 && bstride % kResidualRhs == 0 &&
+                   (reinterpret_cast<uintptr_t>(b) & 15) == 0 &&
+                   (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  if (vec) {
+    dim3 g = grid1d(int64_t(n) * (k / kResidualRhs), P->nbatch);
+    if (kResidualRhs == 2)
+      k_residual_vec<2><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
+                                                P->resid_bits);
+    else
+      k_residual_vec<4><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
+                                                P->resid_bits);
+  } else {
+    dim3 g = grid1d(int64_t(n) * k, P->nbatch);
+    k_residual<<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
+                                       P->resid_bits);
+  }
   return cudaGetLastError();
 }
 
