@@ -14,12 +14,13 @@
 // atomics, so the destination rows of the two inverse products are cleared
 // before the pass that writes them (see solve.cu).  tcgen05.mma kind::tf32
 // with the 3xTF32 split (hi*hi + hi*lo + lo*hi: Markidis et al. 2018; Ootomo
-// and Yokota 2022) accumulates in TMEM; operands are staged through registers
-// (the split needs them there) into shared memory; the loads of stage i+1
-// are issued before the MMAs of stage i.  The kernel runs 256 threads with
-// one 106 KB stage so that two CTAs share an SM and overlap each other's
-// load latency and fixed per-task cost; measured on B200 this beats one CTA
-// of 512 threads with a two-stage ring at every level of the tree.
+// and Yokota 2022) accumulates in TMEM.  Operands move in K stages of 16:
+// cp.async copies the float32 values of stage i+2 into a two-deep raw ring
+// in shared memory while stage i is split into the hi/lo operands and
+// multiplied, so the global-memory latency of two stages is hidden without
+// holding operands in registers.  256 threads per CTA and about 102 KB of
+// shared memory let two CTAs share an SM and overlap each other's fixed
+// per-task cost.
 #include <cuda_runtime.h>
 
 #include "dct_internal.h"
@@ -28,7 +29,7 @@
 namespace dct {
 namespace {
 
-constexpr int kStK = 32;                     // K per pipeline stage
+constexpr int kStK = 16;                     // K per pipeline stage
 #ifndef DCT_TC_RHS
 #define DCT_TC_RHS 256
 #endif
@@ -36,24 +37,47 @@ constexpr int kStK = 32;                     // K per pipeline stage
 #define DCT_TC_CTAS_PER_SM 2
 #endif
 constexpr int kStN = DCT_TC_RHS;             // right-hand sides per CTA
-// A operand (128 x 32): K-adjacent core matrices 160 B apart, so that the
-// transposed loaders (2 rows x 16 K per warp instruction) and the natural
-// ones (8 rows x 4 K) both store to 32 distinct banks.
-constexpr uint32_t kALbo = 160, kASbo = 7 * kALbo + 128;      // 1248
-constexpr int kABytes = (kTcM / 8) * kASbo;                    // 19968
-// B operand (32 K x 256 N), K-major: N-groups of 8 kBSbo = 1040 B apart (one
-// 16 B slot of skew per group, so that the scalar stores of a warp that holds
-// 8 consecutive float4 along N for 4 rows hit distinct banks)
-constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo + 16;   // 1040
-constexpr int kBBytes = (kStN / 8) * kBSbo;                         // 33280
-constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
-constexpr int kNT = 256;       // threads per CTA
-constexpr int kRing = 1;       // shared-memory stages
-constexpr size_t kSolveTcSmem = kRing * size_t(kStageBytes) + 64;
+constexpr int kNT = 256;                     // threads per CTA
+// split A operand (128 x 16), K-major: K-adjacent core matrices 160 B apart,
+// so that the transposed converters (2 rows x 16 K per warp instruction) and
+// the natural ones (8 rows x 4 K) both store to 32 distinct banks.
+constexpr uint32_t kALbo = 160, kASbo = (kStK / 4 - 1) * kALbo + 128;   // 608
+constexpr int kABytes = (kTcM / 8) * kASbo;                             // 9728
+// split B operand (16 K x 256 N), K-major: N-groups of 8 kBSbo = 528 B apart
+// (one 16 B slot of skew per group, so that the scalar stores of a warp that
+// holds 8 consecutive float4 along N for 4 rows hit distinct banks)
+constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo + 16;       // 528
+constexpr int kBBytes = (kStN / 8) * kBSbo;                            // 16896
+constexpr int kSplitBytes = 2 * kABytes + 2 * kBBytes;
+// raw float32 stages as copied: A natural [k][m] with rows of kRawAld
+// floats, A transposed [m][k] with rows of kStK floats, B [k][n] with rows of
+// kRawBld floats (the padding keeps the converters' reads conflict-free)
+constexpr int kRaw = 2;
+constexpr int kRawAld = kTcM + 8;
+constexpr int kRawABytes = kStK * kRawAld * 4;
+constexpr int kRawBld = kStN + 8;
+constexpr int kRawBBytes = kStK * kRawBld * 4;
+constexpr int kRawBytes = kRawABytes + kRawBBytes;
+constexpr size_t kSolveTcSmem = kSplitBytes + kRaw * size_t(kRawBytes) + 64;
 constexpr int kCtasPerSm = DCT_TC_CTAS_PER_SM;
 static_assert(kCtasPerSm * (kSolveTcSmem + 1024) <= 233472, "CTAs per SM");
+static_assert(kRawABytes >= kTcM * kStK * 4, "raw A holds both layouts");
 static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
-                  kBBytes % 16 == 0, "descriptor alignment");
+                  kBBytes % 16 == 0 && kRawABytes % 16 == 0 && (kRawBld * 4) % 16 == 0,
+              "descriptor and copy alignment");
+
+// cp.async of 4 or 16 bytes; src_bytes = 0 fills the destination with zeros
+// and reads nothing
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
 
 enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
 
@@ -64,8 +88,8 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   constexpr int kWarps = kNT / 32;
   static_assert(kWarps % 4 == 0, "whole warpgroups: TMEM lane quarters");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kRing * kStageBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kRing);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kSplitBytes + kRaw * kRawBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
   const PanelTask tk = g.tasks[blockIdx.x];
   const int b = blockIdx.y / g.nchunk;
   const int j0 = (blockIdx.y % g.nchunk) * kStN;
@@ -99,8 +123,7 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) tmem_alloc(tmem_slot, kStN);
-  if (tid == 0)
-    for (int i = 0; i < kRing; ++i) mbar_init(&mbar[i]);
+  if (tid == 0) mbar_init(&mbar[0]);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -108,21 +131,78 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   const uint32_t idesc = umma_idesc_tf32(kTcM, np);
   const int nst = (k1 - k0 + kStK - 1) / kStK;
   bool ok = true;
-  // operand registers: stage st + 1 is loaded while the MMAs of stage st run
-  constexpr int kPerA = (kTcM * kStK / 32) / kWarps;          // 16
-  constexpr int kPerB = kStN * kStK / 4 / kNT;                // 8 float4 (256 columns)
-  float va[kPerA];
-  float4 vb[kPerB];
+  unsigned char* Ahi = smem_raw;
+  unsigned char* Alo = Ahi + kABytes;
+  unsigned char* Bhi = Alo + kABytes;
+  unsigned char* Blo = Bhi + kBBytes;
+  constexpr int kPerA = kTcM * kStK / kNT;          // 8 values
+  constexpr int kPerB = kStN * kStK / 4 / kNT;      // 4 float4
   const bool vec4 = (g.k & 3) == 0;   // 16-byte aligned rows
-  // quad u of this thread: rows kl = 4 (chunk / kNc) + lane % 4, quads
-  // n = 4 (8 (chunk % kNc) + lane / 4): chunks of 4 rows x 32 columns
-  constexpr int kNc = kStN / 32;
-  auto b_coord = [&](int u, int& n, int& kl) {
-    const int c = warp + u * kWarps;           // 0 .. 8 kNc - 1
-    kl = (c / kNc) * 4 + (lane & 3);
-    n = ((c % kNc) * 8 + (lane >> 2)) * 4;
+  // stage st's float32 values -> raw slot st % kRaw (one commit group)
+  auto issue_stage = [&](int st) {
+    unsigned char* raw = smem_raw + kSplitBytes + (st % kRaw) * kRawBytes;
+    float* rA = reinterpret_cast<float*>(raw);
+    float* rB = reinterpret_cast<float*>(raw + kRawABytes);
+    const int kb = k0 + st * kStK;
+    const int kw = min(kStK, k1 - kb);
+#pragma unroll
+    for (int u = 0; u < kPerA; ++u) {
+      const int e = tid + u * kNT;
+      int m, kl, d;
+      if constexpr (kTrans) {
+        m = e / kStK;
+        kl = e % kStK;
+        d = m * kStK + kl;
+      } else {
+        kl = e / kTcM;
+        m = e % kTcM;
+        d = kl * kRawAld + m;
+      }
+      const int kg = kb + kl;
+      bool valid = m < mvalid && kl < kw;
+      if constexpr (MODE == kModeFwdLinv) valid = valid && kg <= m0 + m;
+      if constexpr (MODE == kModeBwdLinv) valid = valid && kg >= m0 + m;
+      const int64_t idx = kTrans ? (roff + kg) + int64_t(m0 + m) * ld
+                                 : (roff + m) + int64_t(kg) * ld;
+      cp_async4(rA + d, valid ? M + idx : M, valid ? 4 : 0);
+    }
+    if (vec4) {
+      // whole 16-byte quads: kc is a multiple of 4 when k is
+#pragma unroll
+      for (int u = 0; u < kStK * kStN / 4 / kNT; ++u) {
+        const int q = tid + u * kNT;
+        const int kl = q / (kStN / 4), n = (q % (kStN / 4)) * 4;
+        const bool valid = kl < kw && n < kc;
+        const float* src = X;
+        if (valid) {
+          const int kg = kb + kl;
+          const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
+                                                   : int64_t(first + kg);
+          src = X + row * g.k + j0 + n;
+        }
+        cp_async16(rB + kl * kRawBld + n, src, valid ? 16 : 0);
+      }
+    } else {
+#pragma unroll 4
+      for (int u = 0; u < kStK * kStN / kNT; ++u) {
+        const int q = tid + u * kNT;
+        const int kl = q / kStN, n = q % kStN;
+        const bool valid = kl < kw && n < kc;
+        const float* src = X;
+        if (valid) {
+          const int kg = kb + kl;
+          const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
+                                                   : int64_t(first + kg);
+          src = X + row * g.k + j0 + n;
+        }
+        cp_async4(rB + kl * kRawBld + n, src, valid ? 4 : 0);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  // element (m, kl) of A handled in slot u (fixed over the stages)
+  // split slots of this thread: A element (m, kl) of slot u; B quad u with
+  // rows kl = 4 (chunk / kNc) + lane % 4 and n = 4 (8 (chunk % kNc) + lane / 4)
+  constexpr int kNc = kStN / 32;
   auto a_coord = [&](int u, int& m, int& kl) {
     const int gi = warp + u * kWarps;
     if constexpr (kTrans) {
@@ -133,75 +213,48 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
       kl = (gi / (kTcM / 8)) * 4 + (lane & 3);
     }
   };
-  auto load_stage = [&](int st) {
-    const int kb = k0 + st * kStK;
-    const int kw = min(kStK, k1 - kb);
-#pragma unroll
-    for (int u = 0; u < kPerA; ++u) {
-      int m, kl;
-      a_coord(u, m, kl);
-      const int kg = kb + kl;
-      bool valid = m < mvalid && kl < kw;
-      if constexpr (MODE == kModeFwdLinv) valid = valid && kg <= m0 + m;
-      if constexpr (MODE == kModeBwdLinv) valid = valid && kg >= m0 + m;
-      const int64_t idx = kTrans ? (roff + kg) + int64_t(m0 + m) * ld
-                                 : (roff + m) + int64_t(kg) * ld;
-      va[u] = valid ? __ldg(M + idx) : 0.0f;
-    }
-    // B: 4 consecutive right-hand sides of one row per slot (a float4 when
-    // the rows are 16-byte aligned); a warp holds 8 consecutive quads of N
-    // (32 right-hand sides) for 4 consecutive rows
-#pragma unroll
-    for (int u = 0; u < kPerB; ++u) {
-      int n, kl;
-      b_coord(u, n, kl);
-      float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (kl < kw && n < kc) {
-        const int kg = kb + kl;
-        const int64_t row = MODE == kModeBwdGemm ? int64_t(__ldg(rows + ns + kg))
-                                                 : int64_t(first + kg);
-        const float* src = X + row * g.k + j0 + n;
-        if (vec4 && n + 4 <= kc) {
-          val = *reinterpret_cast<const float4*>(src);
-        } else {
-          val.x = src[0];
-          if (n + 1 < kc) val.y = src[1];
-          if (n + 2 < kc) val.z = src[2];
-          if (n + 3 < kc) val.w = src[3];
-        }
-      }
-      vb[u] = val;
-    }
+  auto b_coord = [&](int u, int& n, int& kl) {
+    const int c = warp + u * kWarps;
+    kl = (c / kNc) * 4 + (lane & 3);
+    n = ((c % kNc) * 8 + (lane >> 2)) * 4;
   };
-  if (nst > 0) load_stage(0);
+  if (nst > 0) issue_stage(0);
+  if (nst > 1) issue_stage(1);
   for (int st = 0; st < nst; ++st) {
-    const int buf = st % kRing;
-    // the ring slot is free once the MMAs of stage st - kRing have completed
-    if (st >= kRing) {
-      ok = tc_wait(&mbar[buf], uint32_t((st - kRing) / kRing) & 1u, g.status,
-                   DCT_ERR_DEVICE_TIMEOUT, s, b);
+    // this thread's copies of stage st have landed ...
+    if (st + 1 < nst)
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // ... and everyone's (the barrier), and the MMAs of stage st - 1, which
+    // read the split operands, have completed
+    if (st >= 1) {
+      ok = tc_wait(&mbar[0], uint32_t(st - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
       if (!ok) break;
+    } else {
+      __syncthreads();
     }
-    unsigned char* Ahi = smem_raw + buf * kStageBytes;
-    unsigned char* Alo = Ahi + kABytes;
-    unsigned char* Bhi = Alo + kABytes;
-    unsigned char* Blo = Bhi + kBBytes;
+    const unsigned char* raw = smem_raw + kSplitBytes + (st % kRaw) * kRawBytes;
+    const float* rA = reinterpret_cast<const float*>(raw);
+    const float* rB = reinterpret_cast<const float*>(raw + kRawABytes);
     const int kw = min(kStK, k1 - (k0 + st * kStK));
 #pragma unroll
     for (int u = 0; u < kPerA; ++u) {
       int m, kl;
       a_coord(u, m, kl);
+      const float v = kTrans ? rA[m * kStK + kl] : rA[kl * kRawAld + m];
       tc_store_split(Ahi, Alo,
                      uint32_t(m >> 3) * kASbo + uint32_t(kl >> 2) * kALbo +
                          uint32_t(m & 7) * 16 + uint32_t(kl & 3) * 4,
-                     va[u]);
+                     v);
     }
 #pragma unroll
     for (int u = 0; u < kPerB; ++u) {
       int n, kl;
       b_coord(u, n, kl);
       if (n < np) {   // columns at or beyond np are never read
-        const float vv[4] = {vb[u].x, vb[u].y, vb[u].z, vb[u].w};
+        const float4 q4 = *reinterpret_cast<const float4*>(rB + kl * kRawBld + n);
+        const float vv[4] = {q4.x, q4.y, q4.z, q4.w};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int nq = n + q;
@@ -212,7 +265,7 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
         }
       }
     }
-    if (st + 1 < nst) load_stage(st + 1);
+    // after this barrier no thread reads raw slot st % kRaw any more
     tc_publish_smem();
     if (tid == 0) {
       const uint32_t ah = smem_u32(Ahi), al = smem_u32(Alo);
@@ -226,13 +279,16 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
         umma_tf32(tmem, dah, dbl, idesc, 1u);
         umma_tf32(tmem, dal, dbh, idesc, 1u);
       }
-      umma_commit(&mbar[buf]);
+      umma_commit(&mbar[0]);
     }
+    // the next copies after the MMA issue: gathered rows wait on an index load
+    if (st + 2 < nst) issue_stage(st + 2);
   }
+  // no copy may still be writing this CTA's shared memory when it exits
+  asm volatile("cp.async.wait_all;" ::: "memory");
   // the last commit tracks every MMA issued before it
   if (ok && nst > 0)
-    ok = tc_wait(&mbar[(nst - 1) % kRing], uint32_t((nst - 1) / kRing) & 1u, g.status,
-                 DCT_ERR_DEVICE_TIMEOUT, s, b);
+    ok = tc_wait(&mbar[0], uint32_t(nst - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
   if (ok && nst > 0) {
     const int m = (warp & 3) * 32 + lane;
     float* dst = nullptr;
