@@ -60,8 +60,15 @@ constexpr int kRawBBytes = kStK * kRawBld * 4;
 constexpr int kRawBytes = kRawABytes + kRawBBytes;
 constexpr size_t kSolveTcSmem = kSplitBytes + kRaw * size_t(kRawBytes) + 64;
 constexpr int kCtasPerSm = DCT_TC_CTAS_PER_SM;
+// output rows leave by bulk reductions (1) or float atomics (0)
+#ifndef DCT_TC_BULK_REDUCE
+#define DCT_TC_BULK_REDUCE 1
+#endif
+constexpr bool kTcBulkReduce = DCT_TC_BULK_REDUCE != 0;
 static_assert(kCtasPerSm * (kSolveTcSmem + 1024) <= 233472, "CTAs per SM");
 static_assert(kRawABytes >= kTcM * kStK * 4, "raw A holds both layouts");
+static_assert(64 * (kStN + 4) * 4 <= kSplitBytes + kRaw * kRawBytes,
+              "64 staged output rows fit in the operand buffers");
 static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
                   kBBytes % 16 == 0 && kRawABytes % 16 == 0 && (kRawBld * 4) % 16 == 0,
               "descriptor and copy alignment");
@@ -289,7 +296,54 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   // the last commit tracks every MMA issued before it
   if (ok && nst > 0)
     ok = tc_wait(&mbar[0], uint32_t(nst - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
-  if (ok && nst > 0) {
+  const float sgn = kInv ? 1.0f : -1.0f;
+  // rows 16-byte aligned and kc a multiple of 4: every output row of the
+  // tile goes out as one bulk reduction (cp.reduce.async.bulk .add.f32) from
+  // a staging copy in shared memory -- the operand buffers, free once the
+  // last MMA has completed -- instead of kc / 4 vector atomics per row.
+  const bool bulk = kTcBulkReduce && (g.k & 3) == 0;
+  if (ok && nst > 0 && bulk) {
+    float* stage = reinterpret_cast<float*>(smem_raw);
+    // row stride: a multiple of 4 floats with stride / 4 odd, so that the
+    // float4 stores of 8 consecutive rows hit distinct banks
+    int ld = (kc + 3) & ~3;
+    if (((ld >> 2) & 1) == 0) ld += 4;
+    // two rounds of 64 tile rows (TMEM lane quarters 2r and 2r + 1)
+    for (int r = 0; r < 2; ++r) {
+      if (((warp & 3) >> 1) == r) {
+        const int lr = (warp & 1) * 32 + lane;   // staging row
+        for (int cb = (warp >> 2) * 32; cb < np; cb += (kWarps / 4) * 32) {
+          uint32_t v[32];
+          tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
+#pragma unroll
+          for (int c = 0; c < 32; c += 4)
+            if (cb + c < kc)
+              *reinterpret_cast<float4*>(stage + lr * ld + cb + c) =
+                  make_float4(sgn * __uint_as_float(v[c]), sgn * __uint_as_float(v[c + 1]),
+                              sgn * __uint_as_float(v[c + 2]), sgn * __uint_as_float(v[c + 3]));
+        }
+      }
+      // generic-proxy stores -> the bulk copy engine, then everyone's rows
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid < 64) {
+        const int m = 64 * r + tid;
+        if (m < mvalid) {
+          const int64_t row = MODE == kModeFwdBnd ? int64_t(rows[ns + m0 + m])
+                                                  : int64_t(first + m0 + m);
+          asm volatile(
+              "cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f32 [%0], [%1], %2;" ::"l"(
+                  Y + row * g.k + j0),
+              "r"(smem_u32(stage + tid * ld)), "r"(uint32_t(kc) * 4u)
+              : "memory");
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        // the staging rows are read before they are rewritten or released
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      }
+      __syncthreads();
+    }
+  } else if (ok && nst > 0) {
     const int m = (warp & 3) * 32 + lane;
     float* dst = nullptr;
     if (m < mvalid) {
@@ -297,15 +351,13 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
                                               : int64_t(first + m0 + m);
       dst = Y + row * g.k + j0;
     }
-    const float sgn = kInv ? 1.0f : -1.0f;
-    const bool vec = (g.k & 3) == 0;   // 16-byte aligned rows
     for (int cb = (warp >> 2) * 32; cb < np; cb += (kWarps / 4) * 32) {
       uint32_t v[32];
       tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
       if (dst != nullptr) {
 #pragma unroll
         for (int c = 0; c < 32; c += 4) {
-          if (vec && cb + c + 4 <= kc) {
+          if (cb + c + 4 <= kc && (g.k & 3) == 0) {
             atomicAdd(reinterpret_cast<float4*>(dst + cb + c),
                       make_float4(sgn * __uint_as_float(v[c]), sgn * __uint_as_float(v[c + 1]),
                                   sgn * __uint_as_float(v[c + 2]),

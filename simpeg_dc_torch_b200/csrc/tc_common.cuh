@@ -115,17 +115,31 @@ __device__ __forceinline__ void umma_3xtf32(uint32_t tmem, uint32_t a_hi, uint32
 }
 
 // try_wait that may suspend the thread for up to kTcSuspendNs while the phase
-// is incomplete (it returns as soon as the phase completes)
-constexpr uint32_t kTcSuspendNs = 2000;
+// is incomplete (it returns as soon as the phase completes); 0 = the form
+// without a time hint (a system-dependent bound)
+#ifndef DCT_TC_SUSPEND_NS
+#define DCT_TC_SUSPEND_NS 2000
+#endif
+constexpr uint32_t kTcSuspendNs = DCT_TC_SUSPEND_NS;
 __device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity) {
   uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred P1;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
-      "selp.b32 %0, 1, 0, P1;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity), "r"(kTcSuspendNs)
-      : "memory");
+  if constexpr (kTcSuspendNs > 0) {
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(kTcSuspendNs)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  }
   return ok != 0;
 }
 
