@@ -100,6 +100,35 @@ __host__ __device__ inline UpdateRange update_range(int p, int ns, int N, int bp
   return r;
 }
 
+// Programmatic dependent launch for the long chains of dependent launches
+// (panel TRSM <-> trailing update, the substitution products): a kernel
+// launched with launch_pdl may be scheduled while its predecessor in the
+// stream is still running, so it must call pdl_wait() before it touches
+// memory that earlier work writes; pdl_trigger() lets this kernel's own
+// successor be scheduled early.  Without the attribute both are no-ops.
+#ifndef DCT_PDL
+#define DCT_PDL 1
+#endif
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = DCT_PDL ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 struct Schedule {
   std::vector<PanelTask> tasks;    // host copy
   PanelTask* d_tasks = nullptr;    // device copy

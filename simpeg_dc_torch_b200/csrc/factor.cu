@@ -412,6 +412,8 @@ __global__ void __launch_bounds__(kThreads)
 k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
               int64_t front_stride, const T* dinv, const int64_t* dinv_off,
               int64_t dinv_stride) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);   // [q][c] = Dinv[c, q]
   T* S2 = S1 + kPanel * kPanel;              // [q][r] = F[r, q]
@@ -463,6 +465,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
                int64_t front_stride, T* dinv, const int64_t* dinv_off,
                int64_t dinv_stride, int* status) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);   // [k][row of tile i], ld 64
   T* Bs = As + kPanel * kUT;                // [k][row of tile j], ld 64
@@ -554,6 +558,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
                   int64_t front_stride, float* dinv, const int64_t* dinv_off,
                   int64_t dinv_stride, int bpan, int* status) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
   // dynamic shared memory is 16-byte aligned, all the descriptors need;
   // addressing it directly keeps the accesses in the shared state space
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -930,21 +936,23 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                                                          P->front_stride);
         break;
       case kLargePanel:
-        k_large_panel<T><<<grid, kThreads, panel_smem, st>>>(
-            P->ds, t, fronts, P->front_stride, static_cast<const T*>(P->dinv),
-            P->d_dinv_off, P->dinv_stride);
+        e = launch_pdl(k_large_panel<T>, grid, dim3(kThreads), panel_smem, st, P->ds, t, fronts,
+                       P->front_stride, static_cast<const T*>(P->dinv), P->d_dinv_off,
+                       P->dinv_stride);
+        if (e != cudaSuccess) return e;
         break;
       case kLargeUpdate:
         if constexpr (sizeof(T) == 4) {
-          k_large_update_tc<<<grid, kTcThreads, kTcSmem, st>>>(
-              P->ds, t, reinterpret_cast<float*>(fronts), P->front_stride,
-              static_cast<float*>(P->dinv), P->d_dinv_off, P->dinv_stride,
-              P->update_bpan, P->status);
+          e = launch_pdl(k_large_update_tc, grid, dim3(kTcThreads), kTcSmem, st, P->ds, t,
+                         reinterpret_cast<float*>(fronts), P->front_stride,
+                         static_cast<float*>(P->dinv), P->d_dinv_off, P->dinv_stride,
+                         P->update_bpan, P->status);
         } else {
-          k_large_update<T><<<grid, kThreads, update_smem, st>>>(
-              P->ds, t, fronts, P->front_stride, static_cast<T*>(P->dinv),
-              P->d_dinv_off, P->dinv_stride, P->status);
+          e = launch_pdl(k_large_update<T>, grid, dim3(kThreads), update_smem, st, P->ds, t,
+                         fronts, P->front_stride, static_cast<T*>(P->dinv), P->d_dinv_off,
+                         P->dinv_stride, P->status);
         }
+        if (e != cudaSuccess) return e;
         break;
       default:
         return cudaErrorInvalidValue;

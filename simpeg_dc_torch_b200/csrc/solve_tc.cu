@@ -90,6 +90,8 @@ enum TcMode { kModeFwdLinv = 0, kModeFwdBnd, kModeBwdGemm, kModeBwdLinv };
 
 template <int MODE>
 __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
   constexpr bool kTrans = MODE == kModeBwdGemm || MODE == kModeBwdLinv;
   constexpr bool kInv = MODE == kModeFwdLinv || MODE == kModeBwdLinv;
   constexpr int kWarps = kNT / 32;
@@ -395,12 +397,11 @@ cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g0, int64_t count,
                                        static_cast<int>(kSolveTcSmem));
   if (e != cudaSuccess) return e;
   switch (kind) {
-    case kFwdLinvTc: k_solve_tc<kModeFwdLinv><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
-    case kFwdBndTc: k_solve_tc<kModeFwdBnd><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
-    case kBwdGemmTc: k_solve_tc<kModeBwdGemm><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
-    default: k_solve_tc<kModeBwdLinv><<<grid, kNT, kSolveTcSmem, st>>>(g); break;
+    case kFwdLinvTc: return launch_pdl(k_solve_tc<kModeFwdLinv>, grid, dim3(kNT), kSolveTcSmem, st, g);
+    case kFwdBndTc: return launch_pdl(k_solve_tc<kModeFwdBnd>, grid, dim3(kNT), kSolveTcSmem, st, g);
+    case kBwdGemmTc: return launch_pdl(k_solve_tc<kModeBwdGemm>, grid, dim3(kNT), kSolveTcSmem, st, g);
+    default: return launch_pdl(k_solve_tc<kModeBwdLinv>, grid, dim3(kNT), kSolveTcSmem, st, g);
   }
-  return cudaGetLastError();
 }
 
 }  // namespace dct
