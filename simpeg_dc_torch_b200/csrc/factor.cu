@@ -549,6 +549,13 @@ constexpr uint32_t kUpLbo = 128, kUpSbo = (kUpStK / 4) * kUpLbo;   // 1024
 constexpr int kUpOpBytes = (kTcM / 8) * kUpSbo;              // 128 x 32 floats
 constexpr int kUpStageBytes = 4 * kUpOpBytes;                // A hi/lo, B hi/lo
 constexpr int kUpPer = (kTcM / 8) * (kUpStK / 4) / (kTcThreads / 32);   // 8
+// TMEM accumulators: one per panel of a block (a chain of at most kPanel
+// K values each; longer float32 accumulation chains inside the tensor core
+// measurably lose accuracy), all 512 columns of the SM's TMEM -- one CTA
+// per SM
+constexpr int kUpAcc = 4;
+constexpr int kUpTmemCols = kUpAcc * kTcN;
+static_assert(kUpTmemCols <= 512, "TMEM columns of one SM");
 
 // task: s, p, t0 = i, t1 = j (i >= j) over 128-row / 128-column tiles of the
 // trailing block after panel p (columns up to update_range's cend), or
@@ -589,7 +596,7 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   const int np = (nj + 15) & ~15;   // MMA N: a multiple of 16
   const int nst = (base - R.ka + kUpStK - 1) / kUpStK;
 
-  if (warp == 0) tmem_alloc(tmem_slot, kTcN);
+  if (warp == 0) tmem_alloc(tmem_slot, kUpTmemCols);
   if (tid == 0) {
     mbar_init(&mbar[0]);
     mbar_init(&mbar[1]);
@@ -651,9 +658,13 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
         const uint64_t dal = umma_desc(al + ko, kUpLbo, kUpSbo);
         const uint64_t dbh = umma_desc(bh + ko, kUpLbo, kUpSbo);
         const uint64_t dbl = umma_desc(bl + ko, kUpLbo, kUpSbo);
-        umma_tf32(tmem, dah, dbh, idesc, (st > 0 || kk > 0) ? 1u : 0u);
-        umma_tf32(tmem, dah, dbl, idesc, 1u);
-        umma_tf32(tmem, dal, dbh, idesc, 1u);
+        // one accumulator (128 TMEM columns) per panel of the K range
+        const int a = min(st * kUpStK / kPanel, kUpAcc - 1);
+        const uint32_t acc = tmem + uint32_t(a * kTcN);
+        const bool fresh = st * kUpStK == a * kPanel && kk == 0;
+        umma_tf32(acc, dah, dbh, idesc, fresh ? 0u : 1u);
+        umma_tf32(acc, dah, dbl, idesc, 1u);
+        umma_tf32(acc, dal, dbh, idesc, 1u);
       }
       umma_commit(&mbar[buf]);
     }
@@ -667,22 +678,29 @@ k_large_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
     const int row = (warp & 3) * 32 + lane;
     const int cb = (warp >> 2) * 32;
     if (cb < np) {
-      uint32_t v[32];
-      tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(cb), v);
-      if (row < ni) {
-        float* dst = F + (ri + row) + int64_t(rj + cb) * N;
-        float cur[32];
+      float* dst = F + (ri + min(row, ni - 1)) + int64_t(rj + cb) * N;
+      float cur[32];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) cur[c] = (cb + c < nj) ? dst[int64_t(c) * N] : 0.0f;
+      for (int c = 0; c < 32; ++c) cur[c] = (row < ni && cb + c < nj) ? dst[int64_t(c) * N] : 0.0f;
+      // the panels' products are subtracted one at a time, each rounded
+      // to float32 as in a panel-by-panel update
+      const int nacc = min((base - R.ka + kPanel - 1) / kPanel, kUpAcc);
+      for (int a = 0; a < nacc; ++a) {
+        uint32_t v[32];
+        tmem_ld32(tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t(a * kTcN + cb), v);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) cur[c] -= __uint_as_float(v[c]);
+      }
+      if (row < ni) {
 #pragma unroll
         for (int c = 0; c < 32; ++c)
-          if (cb + c < nj) dst[int64_t(c) * N] = cur[c] - __uint_as_float(v[c]);
+          if (cb + c < nj) dst[int64_t(c) * N] = cur[c];
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, kTcN);
+  if (warp == 0) tmem_dealloc(tmem, kUpTmemCols);
   if (ok && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
     __syncthreads();   // this CTA's updates of the block are complete
     factor_diag<float, kTcThreads>(F, N, base, min(kPanel, ns - base), sm,
