@@ -141,6 +141,36 @@ def test_float32_solver_with_refinement(cuda):
     assert res < 1e-7
 
 
+@pytest.mark.parametrize("k", [4, 3])
+def test_wide_supernode_blocked_update(cuda, k):
+    """A dense 330 x 330 block coupled to a 2-D grid: a supernode of six
+    64-column panels, so the float32 factorization runs its narrow updates
+    inside a block of four panels and the deferred K = 256 update beyond it
+    (one TMEM accumulator per panel), then a partial second block; k = 4
+    takes the bulk-reduction epilogue of the substitution, k = 3 the
+    atomics.  Float64 and float32 + refinement against scipy."""
+    rng = np.random.default_rng(3)
+    G = rng.standard_normal((330, 330))
+    D = sp.csr_matrix(G @ G.T / 330 + 4 * np.eye(330))
+    L = laplacian(12)
+    C = sp.random(L.shape[0], 330, density=0.02, random_state=4) * 0.05
+    A = sp.bmat([[L + 2 * sp.eye(L.shape[0]), C], [C.T, D]]).tocsr()
+    A = ((A + A.T) * 0.5).tocsr()
+    A.sort_indices()
+    n = A.shape[0]
+    b = rng.standard_normal((n, k))
+    xr = torch.tensor(spla.spsolve(A.tocsc(), b))
+    crow, col = torch.tensor(A.indptr), torch.tensor(A.indices)
+    vals = torch.tensor(A.data, device=cuda)
+    for dtype, refine, tol in ((torch.float64, None, 1e-11), (torch.float32, 2, 1e-7)):
+        slv = DCTSolver(crow, col, n, k, device=cuda, dtype=dtype,
+                        **({} if refine is None else {"refine": refine}))
+        bt = torch.tensor(b, device=cuda, dtype=dtype)
+        x = sparse_solve(vals, bt, slv).double().cpu()
+        assert rel(x, xr) < tol, (dtype, rel(x, xr))
+        slv.check()
+
+
 def test_zero_pivot_is_reported_not_trapped(cuda):
     A = laplacian(8)
     n = A.shape[0]
