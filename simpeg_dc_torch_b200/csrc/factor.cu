@@ -180,6 +180,11 @@ k_zero_lower(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 
 // task: s = parent, t0 = child, t1 = first column of the child's update
 // matrix handled by this CTA (8 columns, one warp each)
+#ifndef DCT_EXTEND_BATCH
+#define DCT_EXTEND_BATCH 4
+#endif
+constexpr int kExtendBatch = DCT_EXTEND_BATCH;
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_large_extend_add(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
@@ -199,20 +204,23 @@ k_large_extend_add(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
   const int32_t* rel = S.rel + S.rel_ptr[c];
   const int64_t dst_col = int64_t(rel[j]) * N;
   const T* src = U + (nsc + j) * int64_t(nc) + nsc;
-  // batches of 4 per lane: loads before stores (F and U share one buffer)
-  for (int i0 = j + lane; i0 < nbc; i0 += 4 * 32) {
-    T sv[4], fv[4];
-    int64_t at[4];
+  // batches of kExtendBatch per lane, loads before stores (F and U share
+  // one buffer); the row map, the child values and then the parent values
+  // of a whole batch are in flight together
+  for (int i0 = j + lane; i0 < nbc; i0 += kExtendBatch * 32) {
+    T sv[kExtendBatch], fv[kExtendBatch];
+    int32_t ri[kExtendBatch];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < kExtendBatch; ++u) {
       const int i = i0 + 32 * u;
-      at[u] = i < nbc ? rel[i] + dst_col : -1;
+      ri[u] = i < nbc ? rel[i] : -1;
       sv[u] = i < nbc ? src[i] : T(0);
-      fv[u] = i < nbc ? F[at[u]] : T(0);
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (at[u] >= 0) F[at[u]] = fv[u] + sv[u];
+    for (int u = 0; u < kExtendBatch; ++u) fv[u] = ri[u] >= 0 ? F[ri[u] + dst_col] : T(0);
+#pragma unroll
+    for (int u = 0; u < kExtendBatch; ++u)
+      if (ri[u] >= 0) F[ri[u] + dst_col] = fv[u] + sv[u];
   }
 }
 

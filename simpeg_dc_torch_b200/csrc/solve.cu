@@ -430,7 +430,7 @@ __global__ void k_convert(const TI* __restrict__ src, int64_t sstride, int64_t c
 }
 
 // ------------------------------------------------------------ refinement
-// right-hand sides per thread of the refinement residual (1, 2 or 4)
+// right-hand sides per thread of the refinement residual (1, 2, 4 or 8)
 #ifndef DCT_RESIDUAL_RHS
 #define DCT_RESIDUAL_RHS 4
 #endif
@@ -475,7 +475,7 @@ __global__ void k_residual(DevSym S, const double* __restrict__ vals,
   }
 }
 
-// The same with RJ = 2 or 4 consecutive right-hand sides per thread (k a
+// The same with RJ = 2, 4 or 8 consecutive right-hand sides per thread (k a
 // multiple of RJ, rows 16-byte aligned): the row's pattern, permutation and
 // values are read once for RJ outputs, and x, b and r move as 16-byte vectors.
 template <int RJ>
@@ -484,7 +484,7 @@ __global__ void k_residual_vec(DevSym S, const double* __restrict__ vals,
                                int64_t bstride, const double* __restrict__ x, int n,
                                int k, float* __restrict__ r32,
                                unsigned long long* __restrict__ maxbits) {
-  static_assert(RJ == 2 || RJ == 4, "two or four right-hand sides per thread");
+  static_assert(RJ == 2 || RJ == 4 || RJ == 8, "2, 4 or 8 right-hand sides per thread");
   const int bb = blockIdx.y;
   const double* V = vals + int64_t(bb) * vals_stride;
   const double* X = x + int64_t(bb) * n * k;
@@ -522,8 +522,10 @@ __global__ void k_residual_vec(DevSym S, const double* __restrict__ vals,
     if constexpr (RJ == 2) {
       *reinterpret_cast<float2*>(R + o) = make_float2(float(acc[0]), float(acc[1]));
     } else {
-      *reinterpret_cast<float4*>(R + o) =
-          make_float4(float(acc[0]), float(acc[1]), float(acc[2]), float(acc[3]));
+#pragma unroll
+      for (int h = 0; h < RJ; h += 4)
+        *reinterpret_cast<float4*>(R + o + h) = make_float4(
+            float(acc[h]), float(acc[h + 1]), float(acc[h + 2]), float(acc[h + 3]));
     }
 #pragma unroll
     for (int h = 0; h < RJ; ++h) rmax = fmax(rmax, fabs(acc[h]));
@@ -702,8 +704,11 @@ cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
     if (kResidualRhs == 2)
       k_residual_vec<2><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
                                                 P->resid_bits);
-    else
+    else if (kResidualRhs == 4)
       k_residual_vec<4><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
+                                                P->resid_bits);
+    else
+      k_residual_vec<8><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
                                                 P->resid_bits);
   } else {
     dim3 g = grid1d(int64_t(n) * k, P->nbatch);
