@@ -9,10 +9,12 @@
 //   kBwdGemmTc  y_s   -= L_Bs^T[cols m, k] x_B[k]           (B <- gathered A)
 //   kBwdLinvTc  x_s   += L_ss^{-T}[cols m, k] y_s[k]        (A <- B rows)
 //
-// A task covers one 128-row tile of the output and a K range [k0, k1); a
-// product whose K range is split over several tasks accumulates with float
-// atomics, so the destination rows of the two inverse products are cleared
-// before the pass that writes them (see solve.cu).  tcgen05.mma kind::tf32
+// A task covers one 128-row tile of the output and a K range [k0, k1); every
+// task adds its product into the destination rows -- one bulk f32 reduction
+// per row (cp.reduce.async.bulk) when the rows are 16-byte aligned, float
+// atomics otherwise -- so K ranges can be split over tasks, and the
+// destination rows of the two inverse products are cleared before the pass
+// that writes them (see solve.cu).  tcgen05.mma kind::tf32
 // with the 3xTF32 split (hi*hi + hi*lo + lo*hi: Markidis et al. 2018; Ootomo
 // and Yokota 2022) accumulates in TMEM.  Operands move in K stages of 16:
 // cp.async copies the float32 values of stage i+2 into a two-deep raw ring
