@@ -69,7 +69,6 @@ constexpr int kSmallFrontF64 = 160;
 constexpr int kSmallFrontF32 = 224;
 constexpr int kThreads = 256;
 constexpr int kRhsChunk = 64;   // right-hand sides per CTA in the solves
-constexpr int kRowGroup = 4;    // 64-row tiles per CTA in forward panel steps
 constexpr int kUpdateTile = 64;   // trailing-update tile (rows = cols)
 // float32 fronts group their panels in blocks of this many for the trailing
 // update (see update_range); float64 fronts update after every panel

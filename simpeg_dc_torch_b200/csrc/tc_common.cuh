@@ -1,13 +1,14 @@
 // tcgen05 (5th-generation tensor core) helpers shared by the float32 factor
 // and solve kernels: shared-memory matrix descriptors for K-major operands
-// without swizzle, TF32 rounding, TMEM allocation, the 3xTF32 MMA issue and a
-// bounded mbarrier wait.
+// without swizzle, TF32 rounding, TMEM allocation, MMA issue and a bounded
+// mbarrier wait.
 //
 // Operand layout (K-major, no swizzle): core matrices of 8 rows x 16 bytes
-// (4 float values); element (m, k) of an operand with 64 values of K lives at
-// byte (m / 8) * kTcSBO + (k / 4) * kTcLBO + (m % 8) * 16 + (k % 4) * 4.
-// One tcgen05.mma of kind::tf32 consumes K = 8, i.e. two core matrices along
-// K, so successive K steps start 2 * kTcLBO bytes further.
+// (4 float values); element (m, k) lives at byte
+// (m / 8) * SBO + (k / 4) * LBO + (m % 8) * 16 + (k % 4) * 4, with the
+// strides chosen by each kernel.  One tcgen05.mma of kind::tf32 consumes
+// K = 8, i.e. two core matrices along K, so successive K steps start 2 * LBO
+// bytes further.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -18,22 +19,14 @@ namespace dct {
 constexpr int kTcM = 128;                 // MMA M (rows of the A operand)
 constexpr int kTcN = 128;                 // MMA N of the trailing update
 constexpr int kTcThreads = 512;
-constexpr uint32_t kTcLBO = 128, kTcSBO = 2048;
-constexpr int kTcOperandBytes = kTcM * 64 * 4;   // 128 rows x 64 K floats
 constexpr uint32_t kTcWaitLimit = 1u << 20;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-  return (uint64_t((saddr >> 4) & 0x3FFF)) |
-         (uint64_t((kTcLBO >> 4) & 0x3FFF) << 16) |
-         (uint64_t((kTcSBO >> 4) & 0x3FFF) << 32) |
-         (uint64_t(1) << 46);                 // descriptor version for sm_100
-}
-
-// the same with explicit core-matrix strides (bytes, multiples of 16)
+// shared-memory matrix descriptor: start address and core-matrix strides
+// (bytes, multiples of 16)
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t((saddr >> 4) & 0x3FFF)) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
          (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
@@ -93,25 +86,6 @@ __device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t da, uint64_t d
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
           tmem),
       "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-// One thread: D (+)= A B^T over ksteps K-steps of 8 with the 3xTF32 split
-// (hi*hi + hi*lo + lo*hi), then commit the MMAs to the mbarrier.
-__device__ __forceinline__ void umma_3xtf32(uint32_t tmem, uint32_t a_hi, uint32_t a_lo,
-                                            uint32_t b_hi, uint32_t b_lo, int ksteps,
-                                            uint32_t idesc, uint32_t accumulate,
-                                            uint64_t* bar) {
-  for (int kk = 0; kk < ksteps; ++kk) {
-    const uint32_t koff = uint32_t(kk) * 2 * kTcLBO;
-    umma_tf32(tmem, umma_desc(a_hi + koff), umma_desc(b_hi + koff), idesc, accumulate);
-    accumulate = 1;
-    umma_tf32(tmem, umma_desc(a_hi + koff), umma_desc(b_lo + koff), idesc, 1);
-    umma_tf32(tmem, umma_desc(a_lo + koff), umma_desc(b_hi + koff), idesc, 1);
-  }
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
 }
 
 // try_wait that may suspend the thread for up to kTcSuspendNs while the phase
