@@ -246,6 +246,18 @@ TENSOR_KINDS = {"trailing_update", "fwd_linv_tc", "fwd_bnd_tc", "bwd_gemm_tc",
                 "bwd_linv_tc"}
 
 
+def max_over_ranks(x, world, device):
+    """The maximum of a per-rank value over all ranks of the job (every rank
+    calls it, in the same order); with one rank, the value itself."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -278,12 +290,8 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x):
+        return max_over_ranks(x, world, dev)
 
     mesh, survey, m_np = build_case(args.workload, seed=rank)
     e32 = make_engine(args.workload, mesh, survey, dev, torch.float32)
@@ -335,7 +343,7 @@ def main():
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         barrier()
-        return max_over_ranks(a.elapsed_time(b) / steps), clocks
+        return rank_max(a.elapsed_time(b) / steps), clocks
 
     sampler = ClockSampler(local)
     ms32, clocks = timed(e32, args.steps, args.warmup, sampler, tag="timed_fp32")
@@ -371,7 +379,7 @@ def main():
         b.record()
         torch.cuda.synchronize()
         barrier()
-        e2e_ms = max_over_ranks(a.elapsed_time(b) / args.steps)
+        e2e_ms = rank_max(a.elapsed_time(b) / args.steps)
         e2e = {"value": e2e_ms, "unit": "ms",
                "h2d_bytes_per_step": (m_h.numel() + dobs_h.numel()
                                       + w_h.numel()) * 8,
