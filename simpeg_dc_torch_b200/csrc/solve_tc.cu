@@ -312,9 +312,10 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
     // float4 stores of 8 consecutive rows hit distinct banks
     int ld = (kc + 3) & ~3;
     if (((ld >> 2) & 1) == 0) ld += 4;
-    // two rounds of 64 tile rows (TMEM lane quarters 2r and 2r + 1)
-    for (int r = 0; r < 2; ++r) {
-      if (((warp & 3) >> 1) == r) {
+    // two rounds of 64 tile rows (TMEM lane quarters 2r and 2r + 1); rounds
+    // and quarters wholly beyond the tile's valid rows are skipped
+    for (int r = 0; r < 2 && 64 * r < mvalid; ++r) {
+      if (((warp & 3) >> 1) == r && (warp & 3) * 32 < mvalid) {
         const int lr = (warp & 1) * 32 + lane;   // staging row
         for (int cb = (warp >> 2) * 32; cb < np; cb += (kWarps / 4) * 32) {
           uint32_t v[32];
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
       }
       __syncthreads();
     }
-  } else if (ok && nst > 0) {
+  } else if (ok && nst > 0 && (warp & 3) * 32 < mvalid) {
     const int m = (warp & 3) * 32 + lane;
     float* dst = nullptr;
     if (m < mvalid) {
