@@ -229,3 +229,36 @@ def rel(a, b):
     a = np.asarray(a, float)
     b = np.asarray(b, float)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def jvec_3d(op, m, u):
+    """J u for the 3-D engine: A dU = -A(dvals) U with dvals = L3 (-sigma u),
+    J u = (Pd dU)[i, sidx_i] (the product of dctorch/ip3d.py:150-163 before
+    its scale)."""
+    d, slv, U = dpred_3d(op, m, return_fields=True)
+    n = op["nN"]
+    dvals = op["L3"] @ (-sigma_of(m) * np.asarray(u, float))
+    rhs = -(sp.csr_matrix((dvals, op["col"], op["crow"]), shape=(n, n)) @ U)
+    dU = slv.solve(rhs[None])[0]
+    PU = op["Pd"] @ dU
+    return PU[np.arange(PU.shape[0]), op["sidx"]]
+
+
+def ip_scale(v_dc, chargeability):
+    """Per-datum IP scale: 1 / V_dc where the receiver's data type is
+    apparent chargeability, else 1 (dctorch/ip2d.py:96-106, ip3d.py:125-135)."""
+    s = np.ones_like(np.asarray(v_dc, float))
+    c = np.asarray(chargeability, bool)
+    s[c] = 1.0 / np.asarray(v_dc, float)[c]
+    return s
+
+
+def ip_dpred_2d(op, m_dc, eta, chargeability):
+    """Linearized 2.5-D IP data scale * J(m_dc) eta (dctorch/ip2d.py:112-133)."""
+    return ip_scale(dpred_2d(op, m_dc), chargeability) * jvec_2d(op, m_dc, eta)
+
+
+def ip_dpred_3d(op, m_dc, eta, chargeability):
+    """Linearized 3-D IP data scale * J(m_dc) eta (dctorch/ip3d.py:150-163)."""
+    return ip_scale(dpred_3d(op, m_dc), chargeability) * jvec_3d(op, m_dc, eta)
+

@@ -21,3 +21,4 @@ from .solver import (CuDSSBatchSolver, CuDSSSolver, DCTBatchSolver,  # noqa: F40
                      sparse_solve_batch, sparse_solve_batch_prefactored)
 from .simulation2d import Linearization2D, TorchDC2D  # noqa: F401
 from .simulation3d import TorchDC3D  # noqa: F401
+from .ip import TorchIP2D, TorchIP3D  # noqa: F401

@@ -8,15 +8,26 @@ can be used in place of these classes.
 Nodal source term (SimPEG `BaseSrc.eval`, EB formulation): the current
 electrode(s) enter the right-hand side through the node interpolation matrix,
 `q = I (P_A - P_B)`, with B absent for a pole.  Receivers read
-`P = P_M - P_N` (dipole) or `P_M` (pole); data type "volt".
+`P = P_M - P_N` (dipole) or `P_M` (pole).  Data type "volt"; a receiver
+of an induced-polarization survey may say "apparent_chargeability" instead,
+which the DC engines read as volts and the IP engines (`ip.py`) scale by the
+background datum, as SimPEG's `BaseIPSimulation._scale` does.
 """
 from __future__ import annotations
 
 import numpy as np
 
 
+_DATA_TYPES = ("volt", "apparent_chargeability")
+
+
 class _Receiver:
     data_type = "volt"
+
+    def _set_type(self, data_type):
+        if data_type not in _DATA_TYPES:
+            raise ValueError(f"data_type must be one of {_DATA_TYPES}")
+        self.data_type = data_type
 
     @property
     def nD(self):
@@ -25,8 +36,7 @@ class _Receiver:
 
 class DipoleReceiver(_Receiver):
     def __init__(self, locations_m, locations_n, data_type="volt"):
-        if data_type != "volt":
-            raise ValueError("only data_type='volt' is supported")
+        self._set_type(data_type)
         self.locations_m = np.atleast_2d(np.asarray(locations_m, float))
         self.locations_n = np.atleast_2d(np.asarray(locations_n, float))
         if self.locations_m.shape != self.locations_n.shape:
@@ -39,8 +49,7 @@ class DipoleReceiver(_Receiver):
 
 class PoleReceiver(_Receiver):
     def __init__(self, locations, data_type="volt"):
-        if data_type != "volt":
-            raise ValueError("only data_type='volt' is supported")
+        self._set_type(data_type)
         self.locations_m = np.atleast_2d(np.asarray(locations, float))
         self.locations_n = None
 

@@ -23,6 +23,12 @@ path in float64:
   dc2d_lin.npz    : on the dc2d_tiny problem, TorchDC2D.Jmatrix and Jvec,
       and Linearization2D's d, Jvec, Jtvec, diag_JtDJ and Jmatrix.
   dc3d_tiny.npz / dc3d_suite.npz : the same for TorchDC3D.
+  ip_tiny.npz     : linearized IP (dctorch/ip2d.py TorchIP2D, ip3d.py
+      TorchIP3D) on the tiny 2-D and 3-D problems with every other receiver
+      of data type "apparent_chargeability": V_dc, the per-datum scale, the
+      IP data and the misfit gradient with respect to eta.  The IP
+      constructors build their DC engine themselves (which needs SimPEG);
+      here that name is pointed at the stub engines above while they run.
 """
 from __future__ import annotations
 
@@ -256,6 +262,65 @@ def main():
                        sidx=ops.sidx)
         np.savez_compressed(os.path.join(out, name + ".npz"), **rec)
         print(name, "nN", ops.nN, "nD", ops.nD)
+
+    np.savez_compressed(os.path.join(out, "ip_tiny.npz"),
+                        **ip_fixture(a.reference, S, Q, S2, S3))
+
+
+def mark_chargeability(survey):
+    """Every other receiver (in survey order) becomes an apparent-
+    chargeability receiver; returns the per-receiver flags."""
+    flags = []
+    for src in survey.source_list:
+        for rx in src.receiver_list:
+            if len(flags) % 2 == 1:
+                rx.data_type = "apparent_chargeability"
+            flags.append(rx.data_type == "apparent_chargeability")
+    return np.array(flags)
+
+
+def ip_fixture(root, S, Q, S2, S3):
+    import dctorch.ip2d as I2
+    import dctorch.ip3d as I3
+    rec = {}
+    for tag, (mesh, survey, m) in (("2d", syn.tiny_2d()), ("3d", syn.tiny_3d())):
+        flags = mark_chargeability(survey)
+        ops = nodal_operators(mesh, survey)
+        if tag == "2d":
+            rmin, rmax = electrode_distance_range(survey)
+            kys, wq, _ = Q.k0_quadrature(rmin, rmax, 7)
+            eng, _ = engine_2d(S2, ops, kys, wq)
+            saved, S2.TorchDC2D = S2.TorchDC2D, (lambda *a, **k: eng)
+            try:
+                ip = I2.TorchIP2D(mesh, survey, m, nky=7, device="cpu",
+                                  dtype=torch.float64, quadrature=(kys, wq))
+            finally:
+                S2.TorchDC2D = saved
+            rec.update(kys=kys, wq=wq)
+        else:
+            eng, _ = engine_3d(S3, S, ops)
+            saved, S3.TorchDC3D = S3.TorchDC3D, (lambda *a, **k: eng)
+            try:
+                ip = I3.TorchIP3D(mesh, survey, m, device="cpu", dtype=torch.float64)
+            finally:
+                S3.TorchDC3D = saved
+        rng = np.random.default_rng(31)
+        eta = rng.uniform(0.0, 0.1, ops.nC)
+        with torch.no_grad():
+            d = ip.dpred(torch.tensor(eta)).numpy()
+        dobs = d * (1.0 + 0.05 * rng.standard_normal(d.size))
+        w = 1.0 / (0.05 * np.abs(dobs) + 1e-3 * np.abs(dobs).max())
+        et = torch.tensor(eta, requires_grad=True)
+        phi = ip.misfit(et, torch.tensor(dobs), torch.tensor(w))
+        phi.backward()
+        rec.update({f"{tag}_m": m, f"{tag}_flags": flags, f"{tag}_eta": eta,
+                    f"{tag}_dobs": dobs, f"{tag}_w": w,
+                    f"{tag}_vdc": ip.v_dc.numpy(), f"{tag}_scale": ip._scale.numpy(),
+                    f"{tag}_d": d, f"{tag}_phi": float(phi),
+                    f"{tag}_grad": et.grad.numpy()})
+        print("ip", tag, "nD", d.size, "chargeability data",
+              int((ip._scale.numpy() != 1.0).sum()))
+    return rec
 
 
 if __name__ == "__main__":

@@ -90,3 +90,38 @@ def test_linearised_products_match_reference():
     # J is the Jacobian of dpred: its rows are the Jtvec of unit data
     u = L["u"]
     assert O.rel(J @ u, L["jvec"]) < 1e-11
+
+
+def _datum_flags(survey, rx_flags):
+    """Per-datum chargeability flags from per-receiver ones (survey order)."""
+    out, i = [], 0
+    for src in survey.source_list:
+        for rx in src.receiver_list:
+            out += [bool(rx_flags[i])] * rx.nD
+            i += 1
+    return np.array(out)
+
+
+def test_ip_forward_matches_reference():
+    """Linearized IP of the oracle (scale * J(m_dc) eta) against the
+    reference's TorchIP2D / TorchIP3D (dctorch/ip2d.py, ip3d.py) on the tiny
+    problems, every other receiver of apparent-chargeability type."""
+    from simpeg_dc_torch_b200 import synthetic as syn
+    ip = golden("ip_tiny")
+    for tag, name, case, three_d in (("2d", "dc2d_tiny", syn.tiny_2d, False),
+                                     ("3d", "dc3d_tiny", syn.tiny_3d, True)):
+        op = _ops(golden(name), three_d)
+        _, survey, _ = case()
+        charge = _datum_flags(survey, ip[f"{tag}_flags"])
+        m, eta = ip[f"{tag}_m"], ip[f"{tag}_eta"]
+        v_dc = O.dpred_3d(op, m) if three_d else O.dpred_2d(op, m)
+        assert O.rel(v_dc, ip[f"{tag}_vdc"]) < 1e-12
+        scale = O.ip_scale(v_dc, charge)
+        assert O.rel(scale, ip[f"{tag}_scale"]) < 1e-12
+        assert charge.any() and (~charge).any()
+        d = (O.ip_dpred_3d if three_d else O.ip_dpred_2d)(op, m, eta, charge)
+        assert O.rel(d, ip[f"{tag}_d"]) < 1e-11
+        w, dobs = ip[f"{tag}_w"], ip[f"{tag}_dobs"]
+        g = 2.0 * w * w * (d - dobs) * scale
+        grad = O.jtvec_3d(op, m, g) if three_d else O.jtvec_2d(op, m, g)
+        assert O.rel(grad, ip[f"{tag}_grad"]) < 1e-10
