@@ -262,3 +262,43 @@ def ip_dpred_3d(op, m_dc, eta, chargeability):
     """Linearized 3-D IP data scale * J(m_dc) eta (dctorch/ip3d.py:150-163)."""
     return ip_scale(dpred_3d(op, m_dc), chargeability) * jvec_3d(op, m_dc, eta)
 
+
+
+def dcip_dpred_2d(op, m_rho, eta, ip_scale=1.0, dc_state="total"):
+    """Joint non-linear DC + IP data (dctorch/dcip2d.py:152-180): V0 at
+    sigma = exp(-m_rho), V1 at sigma (1 - eta); d_IP = ip_scale (V1 - V0) / V1,
+    d_DC = V1 ("total") or V0 ("instantaneous").  Returns (d_DC, d_IP, V0, V1)."""
+    eta = np.asarray(eta, float)
+    v0 = dpred_2d(op, m_rho)
+    v1 = dpred_2d(op, np.asarray(m_rho, float) - np.log1p(-eta))
+    d_dc = v1 if dc_state == "total" else v0
+    return d_dc, ip_scale * (v1 - v0) / v1, v0, v1
+
+
+def dcip_misfit_grad_2d(op, m, eta_max, ip_scale, dc_state, dobs_dc, w_dc,
+                        dobs_ip, w_ip, lam):
+    """(phi, dphi/dm) of the joint misfit for the stacked model
+    m = cat(log-rho, logit(eta / eta_max)) (dctorch/dcip2d.py:182-193), by
+    the chain rule through both states' adjoints."""
+    m = np.asarray(m, float)
+    n = m.size // 2
+    m_rho, m_eta = m[:n], m[n:]
+    s = 1.0 / (1.0 + np.exp(-m_eta))
+    eta = eta_max * s
+    d_dc, d_ip, v0, v1 = dcip_dpred_2d(op, m_rho, eta, ip_scale, dc_state)
+    r_dc = w_dc * (d_dc - dobs_dc)
+    r_ip = w_ip * (d_ip - dobs_ip)
+    phi = float((r_dc ** 2).sum() + lam * (r_ip ** 2).sum())
+    g_dc = 2.0 * w_dc * r_dc
+    g_ip = 2.0 * lam * w_ip * r_ip
+    g0 = -g_ip * ip_scale / v1
+    g1 = g_ip * ip_scale * v0 / v1 ** 2
+    if dc_state == "total":
+        g1 = g1 + g_dc
+    else:
+        g0 = g0 + g_dc
+    m_eff = m_rho - np.log1p(-eta)
+    j1 = jtvec_2d(op, m_eff, g1)
+    grad_rho = jtvec_2d(op, m_rho, g0) + j1
+    grad_eta = j1 / (1.0 - eta) * eta_max * s * (1.0 - s)
+    return phi, np.concatenate([grad_rho, grad_eta])

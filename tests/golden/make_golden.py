@@ -29,6 +29,10 @@ path in float64:
       IP data and the misfit gradient with respect to eta.  The IP
       constructors build their DC engine themselves (which needs SimPEG);
       here that name is pointed at the stub engines above while they run.
+  dcip_tiny.npz   : the joint non-linear DC + IP engine (dctorch/dcip2d.py
+      TorchDCIP2D) on the tiny 2-D problem for both DC states: the DC and
+      IP data of a stacked (log-rho, logit-eta) model and the gradient of
+      its joint misfit.
 """
 from __future__ import annotations
 
@@ -265,6 +269,7 @@ def main():
 
     np.savez_compressed(os.path.join(out, "ip_tiny.npz"),
                         **ip_fixture(a.reference, S, Q, S2, S3))
+    np.savez_compressed(os.path.join(out, "dcip_tiny.npz"), **dcip_fixture(S, Q, S2))
 
 
 def mark_chargeability(survey):
@@ -320,6 +325,44 @@ def ip_fixture(root, S, Q, S2, S3):
                     f"{tag}_grad": et.grad.numpy()})
         print("ip", tag, "nD", d.size, "chargeability data",
               int((ip._scale.numpy() != 1.0).sum()))
+    return rec
+
+
+def dcip_fixture(S, Q, S2):
+    import dctorch.dcip2d as D2
+    mesh, survey, m = syn.tiny_2d()
+    ops = nodal_operators(mesh, survey)
+    rmin, rmax = electrode_distance_range(survey)
+    kys, wq, _ = Q.k0_quadrature(rmin, rmax, 7)
+    rec = dict(kys=kys, wq=wq, m_rho=m)
+    for state in ("total", "instantaneous"):
+        eng, _ = engine_2d(S2, ops, kys, wq)
+        saved, S2.TorchDC2D = S2.TorchDC2D, (lambda *a, **k: eng)
+        try:
+            dcip = D2.TorchDCIP2D(mesh, survey, nky=7, device="cpu",
+                                  dtype=torch.float64, eta_max=0.8,
+                                  ip_scale=1000.0, dc_state=state,
+                                  quadrature=(kys, wq))
+        finally:
+            S2.TorchDC2D = saved
+        rng = np.random.default_rng(41)
+        eta = rng.uniform(0.02, 0.3, ops.nC)
+        mm = np.concatenate([m, dcip.m_eta_of(eta)])
+        with torch.no_grad():
+            d_dc, d_ip = (x.numpy() for x in dcip.dpred(torch.tensor(mm)))
+        dobs_dc = d_dc * (1.0 + 0.03 * rng.standard_normal(d_dc.size))
+        w_dc = 1.0 / (0.03 * np.abs(dobs_dc) + 1e-3 * np.abs(dobs_dc).max())
+        dobs_ip = d_ip + 2.0 * rng.standard_normal(d_ip.size)
+        w_ip = np.full(d_ip.size, 0.5)
+        mt = torch.tensor(mm, requires_grad=True)
+        phi = dcip.misfit(mt, torch.tensor(dobs_dc), torch.tensor(w_dc),
+                          torch.tensor(dobs_ip), torch.tensor(w_ip), lam=0.7)
+        phi.backward()
+        rec.update({f"{state}_m": mm, f"{state}_d_dc": d_dc, f"{state}_d_ip": d_ip,
+                    f"{state}_dobs_dc": dobs_dc, f"{state}_w_dc": w_dc,
+                    f"{state}_dobs_ip": dobs_ip, f"{state}_w_ip": w_ip,
+                    f"{state}_phi": float(phi), f"{state}_grad": mt.grad.numpy()})
+        print("dcip", state, "nD", d_dc.size, "max d_ip", float(np.abs(d_ip).max()))
     return rec
 
 

@@ -1,8 +1,9 @@
-"""Linearized IP engines (TorchIP2D / TorchIP3D) on the GPU against the
-reference's own TorchIP2D / TorchIP3D (golden fixture ip_tiny, made by
-running dctorch/ip2d.py and ip3d.py on the tiny problems with every other
-receiver of apparent-chargeability type): background data V_dc, the
-per-datum scale, the IP data and the misfit gradient with respect to eta.
+"""IP engines on the GPU against the reference's own: the linearized
+TorchIP2D / TorchIP3D (golden fixture ip_tiny, made by running
+dctorch/ip2d.py and ip3d.py on the tiny problems with every other receiver
+of apparent-chargeability type: background data V_dc, the per-datum scale,
+the IP data and the misfit gradient with respect to eta) and the joint
+non-linear TorchDCIP2D (dcip_tiny, dctorch/dcip2d.py, both DC states).
 float64 is held to 1e-10, float32 + refinement to 1e-6 (data) / 1e-5
 (gradient), the levels of the DC engine tests."""
 import numpy as np
@@ -10,7 +11,7 @@ import pytest
 import torch
 
 from conftest import golden
-from simpeg_dc_torch_b200 import TorchIP2D, TorchIP3D
+from simpeg_dc_torch_b200 import TorchDCIP2D, TorchIP2D, TorchIP3D
 from simpeg_dc_torch_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -92,3 +93,46 @@ def test_ip_active_cells(cuda):
     part.misfit(ea, dobs, w).backward()
     assert rel(part.dpred(ea.detach()), full.dpred(ef.detach()).cpu()) < 1e-12
     assert rel(ea.grad, ef.grad[torch.tensor(act, device=cuda)].cpu()) < 1e-12
+
+
+@pytest.mark.parametrize("state", ["total", "instantaneous"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_dcip_matches_reference(cuda, state, dtype):
+    J = golden("dcip_tiny")
+    mesh, survey, _ = syn.tiny_2d()
+    eng = TorchDCIP2D(mesh, survey, nky=7, device=cuda, dtype=dtype, eta_max=0.8,
+                      ip_scale=1000.0, dc_state=state, quadrature=(J["kys"], J["wq"]))
+    tol_d, tol_g = (1e-10, 1e-9) if dtype == torch.float64 else (1e-6, 1e-5)
+    t = lambda k: torch.tensor(J[f"{state}_{k}"], device=cuda)  # noqa: E731
+    mm = torch.tensor(J[f"{state}_m"], device=cuda, requires_grad=True)
+    phi = eng.misfit(mm, t("dobs_dc"), t("w_dc"), t("dobs_ip"), t("w_ip"), lam=0.7)
+    phi.backward()
+    with torch.no_grad():
+        d_dc, d_ip = eng.dpred(mm)
+    assert rel(d_dc, J[f"{state}_d_dc"]) < tol_d
+    assert rel(d_ip, J[f"{state}_d_ip"]) < tol_d
+    assert abs(float(phi) - J[f"{state}_phi"]) <= tol_g * abs(J[f"{state}_phi"])
+    assert rel(mm.grad, J[f"{state}_grad"]) < tol_g
+    eng.check()
+
+
+def test_dcip_active_cells(cuda):
+    """On the active cells, with log-rho val_inactive and eta = 0 elsewhere,
+    the joint data equal those of the full-mesh engine."""
+    J = golden("dcip_tiny")
+    mesh, survey, _ = syn.tiny_2d()
+    n = J["m_rho"].size
+    act = np.random.default_rng(6).uniform(size=n) > 0.3
+    kw = dict(nky=7, device=cuda, eta_max=0.8, ip_scale=1000.0,
+              quadrature=(J["kys"], J["wq"]))
+    full = TorchDCIP2D(mesh, survey, **kw)
+    part = TorchDCIP2D(mesh, survey, active_cells=act, val_inactive=4.0, **kw)
+    m_rho = J["m_rho"].copy()
+    m_rho[~act] = 4.0
+    eta = np.where(act, 0.1, 0.0)
+    df = full.dpred_from_fields(torch.tensor(m_rho, device=cuda), torch.tensor(eta, device=cuda))
+    dp = part.dpred_from_fields(torch.tensor(m_rho[act], device=cuda),
+                                torch.tensor(eta[act], device=cuda))
+    assert rel(dp[0], df[0].cpu()) < 1e-12
+    assert rel(dp[1], df[1].cpu()) < 1e-12
+

@@ -125,3 +125,24 @@ def test_ip_forward_matches_reference():
         g = 2.0 * w * w * (d - dobs) * scale
         grad = O.jtvec_3d(op, m, g) if three_d else O.jtvec_2d(op, m, g)
         assert O.rel(grad, ip[f"{tag}_grad"]) < 1e-10
+
+
+def test_dcip_forward_matches_reference():
+    """The joint non-linear DC + IP forward and misfit gradient of the oracle
+    against the reference's TorchDCIP2D (dctorch/dcip2d.py) on the tiny 2-D
+    problem, both DC states."""
+    g = golden("dc2d_tiny")
+    op = _ops(g, False)
+    J = golden("dcip_tiny")
+    n = J["m_rho"].size
+    for state in ("total", "instantaneous"):
+        mm = J[f"{state}_m"]
+        eta = 0.8 / (1.0 + np.exp(-mm[n:]))
+        d_dc, d_ip, _, _ = O.dcip_dpred_2d(op, mm[:n], eta, 1000.0, state)
+        assert O.rel(d_dc, J[f"{state}_d_dc"]) < 1e-12
+        assert O.rel(d_ip, J[f"{state}_d_ip"]) < 1e-10
+        phi, grad = O.dcip_misfit_grad_2d(
+            op, mm, 0.8, 1000.0, state, J[f"{state}_dobs_dc"], J[f"{state}_w_dc"],
+            J[f"{state}_dobs_ip"], J[f"{state}_w_ip"], 0.7)
+        assert abs(phi - J[f"{state}_phi"]) <= 1e-10 * abs(J[f"{state}_phi"])
+        assert O.rel(grad, J[f"{state}_grad"]) < 1e-9
