@@ -302,3 +302,56 @@ def dcip_misfit_grad_2d(op, m, eta_max, ip_scale, dc_state, dobs_dc, w_dc,
     grad_rho = jtvec_2d(op, m_rho, g0) + j1
     grad_eta = j1 / (1.0 - eta) * eta_max * s * (1.0 - s)
     return phi, np.concatenate([grad_rho, grad_eta])
+
+
+def unit_primary_2d(nodes, kys, poles, radii):
+    """Unit-resistivity half-space primary (dctorch/singularity.py:47-82):
+    K_0(ky r) / pi summed over each source's poles (location, sign), and at
+    a pole's own node the mean of K_0 over a disc of radius R,
+    2 (1 - a K_1(a)) / a^2 / pi with a = ky R.  poles[j] lists the poles of
+    source j, radii[j] the disc radius of each.  Returns (nky, nN, nS)."""
+    from scipy.special import k0, k1
+    nodes = np.asarray(nodes, float)
+    tol = 1e-9 * max(1.0, float(np.abs(nodes).max()))
+    out = np.zeros((len(kys), nodes.shape[0], len(poles)))
+    for j, plist in enumerate(poles):
+        for (loc, sign), R in zip(plist, radii[j]):
+            r = np.sqrt(((nodes - np.asarray(loc, float)[None, :2]) ** 2).sum(1))
+            for ik, ky in enumerate(kys):
+                v = k0(np.maximum(ky * r, 1e-300)) / np.pi
+                at = r < tol
+                if at.any():
+                    a = ky * R
+                    v[at] = 2.0 * (1.0 - a * k1(a)) / a ** 2 / np.pi
+                out[ik, :, j] += sign * v
+    return out
+
+
+def dpred_2d_sr(op, m, u1, return_fields=False):
+    """Singularity-removed data (dctorch/simulation2d.py:316-333): the total
+    field rho_s u_1 + A^{-1}(A(1) u_1 - A(sigma) rho_s u_1), which equals
+    A(sigma)^{-1} A(1) u_1 for any background rho_s."""
+    nky = len(op["wq"])
+    VALS = vals_2d(op["Lstack"], m, nky)
+    ONES = (op["Lstack"] @ np.ones(op["Lstack"].shape[1])).reshape(nky, -1)
+    n = op["nN"]
+    slv = SuperLUBatch(op["crow"], op["col"], n)
+    slv.factorize(VALS)
+    B = np.stack([sp.csr_matrix((ONES[k], op["col"], op["crow"]), shape=(n, n)) @ u1[k]
+                  for k in range(nky)])
+    U = slv.solve(B)
+    Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
+    PU = op["Pd"] @ Ubar
+    d = PU[np.arange(PU.shape[0]), op["sidx"]]
+    if return_fields:
+        return d, VALS, slv, U
+    return d
+
+
+def misfit_grad_2d_sr(op, m, u1, dobs, w):
+    """(phi, dphi/dm) under singularity removal: the right-hand side A(1) u_1
+    does not depend on the model, so the plain adjoint with the total field."""
+    fields = dpred_2d_sr(op, m, u1, return_fields=True)
+    r = w * (fields[0] - dobs)
+    _, g = _adjoint_2d(op, m, 2.0 * w * r, fields)
+    return float((r ** 2).sum()), g

@@ -57,6 +57,7 @@ class FusedPath:
         self.nD = Pd.shape[0]
         dt = torch.float64 if precision == "fp64" else torch.float32
         self.width = int(n_rhs or self.nS)
+        self._pri = None      # singularity-removal split (set_primary)
         self.solver = DCTBatchSolver(crow, col, nN, self.width, self.nbatch,
                                      device=device, dtype=dt, coords=coords,
                                      refine=refine)
@@ -161,6 +162,49 @@ class FusedPath:
         self._plan.set_refinement(self.refine_fields)
         return self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
 
+    # ------------------------------------------------ singularity removal
+    def set_primary(self, u1, vals_one, src_cell, rho_fixed=None):
+        """Use the split u = rho_s u_1 + u_s (see primary.py) for the fields
+        of `forward`: u1 (nbatch, nN, nS) unit primary in node order,
+        vals_one (nbatch, nnzA) the system values at unit conductivity,
+        src_cell (nS,) the cell of each source's A electrode, rho_fixed an
+        optional fixed background."""
+        X = torch.empty((self.nbatch, self.nN, self.nS), dtype=torch.float64,
+                        device=self.device)
+        X[:, self.iperm_d, :] = torch.as_tensor(np.asarray(u1, float), device=self.device)
+        X = X.contiguous()
+        v1 = torch.as_tensor(np.asarray(vals_one, float).reshape(-1),
+                             device=self.device).contiguous()
+        # A(1) u_1 depends on nothing but the geometry: formed once
+        R1 = self._pattern_product(v1, X, 1.0)
+        self._pri = dict(X=X, R1=R1,
+                         cell=torch.as_tensor(np.asarray(src_cell, np.int64),
+                                              device=self.device),
+                         fixed=None if rho_fixed is None else float(rho_fixed))
+
+    def _pattern_product(self, vals, X, alpha):
+        """alpha A(vals) X for every system, X and the result permuted."""
+        Y = torch.empty_like(X)
+        nat.check(nat.lib().dct_pattern_spmm(
+            self.nbatch, self.nN, X.shape[-1], self.solver.crow.data_ptr(),
+            self.col_e.data_ptr(), self._iperm_ptr, vals.data_ptr(), self.nnzA,
+            float(alpha), X.data_ptr(), Y.data_ptr(), self._st()), "dct_pattern_spmm")
+        return Y
+
+    def _fields_split(self, m_full, vals):
+        """U = rho_s u_1 + A^{-1} (A(1) u_1 - A(sigma) rho_s u_1), permuted."""
+        p = self._pri
+        if p["fixed"] is not None:
+            rho = torch.full((self.nS,), p["fixed"], dtype=torch.float64, device=self.device)
+        else:
+            rho = torch.exp(m_full.detach().to(self.device, torch.float64)[p["cell"]])
+        Xs = (p["X"] * rho.view(1, 1, -1)).contiguous()
+        rhs = p["R1"] + self._pattern_product(vals.reshape(-1).contiguous(), Xs, -1.0)
+        self._plan.set_refinement(self.refine_fields)
+        Us = torch.empty_like(rhs)
+        self._plan.solve_permuted(rhs.data_ptr(), 1, self.nS, Us.data_ptr(), self._st())
+        return Xs + Us
+
     def project(self, U):
         d = torch.empty(self.nD, dtype=torch.float64, device=self.device)
         nat.check(nat.lib().dct_project_data(
@@ -176,7 +220,7 @@ class FusedPath:
         solver stamp of the factorization they were computed with."""
         sigma, vals = self.values(m_full)
         self.factorize(vals)
-        U = self.fields()
+        U = self.fields() if self._pri is None else self._fields_split(m_full, vals)
         d = self.project(U)
         return d, sigma, U, self.solver.stamp
 

@@ -129,6 +129,27 @@ class TensorMesh:
             v = np.multiply.outer(v, self.h[ax])
         return v.reshape(-1, order="F")
 
+    @property
+    def h_gridded(self):
+        """Cell widths (nC, dim), cell order (first axis fastest)."""
+        g = np.meshgrid(*self.h, indexing="ij")
+        return np.column_stack([x.reshape(-1, order="F") for x in g])
+
+    def point2index(self, locs):
+        """Index of the cell holding each point (nP, dim): along each axis the
+        cell [x_i, x_{i+1}) that contains the coordinate, the last cell for
+        the far boundary."""
+        locs = np.atleast_2d(np.asarray(locs, float))
+        idx = np.zeros(locs.shape[0], dtype=np.int64)
+        stride = 1
+        for ax in range(self.dim):
+            nodes = self._axis_nodes(ax)
+            i = np.searchsorted(nodes, locs[:, ax], side="right") - 1
+            i = np.clip(i, 0, len(self.h[ax]) - 1)
+            idx += i * stride
+            stride *= len(self.h[ax])
+        return idx
+
     def node_grid_index(self):
         """Integer (i, j[, k]) grid coordinates of every node, node order."""
         g = np.meshgrid(*[np.arange(n) for n in self.shape_nodes],

@@ -25,6 +25,7 @@ import numpy as np
 import scipy.sparse as sp
 import torch
 
+from .primary import source_cells, unit_primary
 from ._fused import FusedDpred, FusedPath
 from .operators import nodal_operators
 from .quadrature import (amplification, electrode_distance_range,
@@ -72,9 +73,6 @@ class TorchDC2D:
                  dtype=torch.float64, active_cells=None, val_inactive=None,
                  chunk=None, singularity_removal=False, rho_primary=None,
                  quadrature=None, refine=None, refine_fields=None):
-        if singularity_removal:
-            raise NotImplementedError(
-                "singularity removal is not part of this implementation")
         if quadrature is None:
             quadrature = os.environ.get("DCTORCH_QUADRATURE", "electrodes")
         if isinstance(quadrature, str) and quadrature != "electrodes":
@@ -88,7 +86,8 @@ class TorchDC2D:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.dtype = dtype
         self.chunk = None if chunk is None else int(chunk)
-        self._sr = False
+        self._sr = bool(singularity_removal)
+        self._rho_p = None if rho_primary is None else float(rho_primary)
 
         rmin, rmax = electrode_distance_range(survey)
         if isinstance(quadrature, str):
@@ -123,6 +122,13 @@ class TorchDC2D:
                                if hasattr(mesh, "node_grid_index") else None,
                                refine=refine, refine_fields=refine_fields)
         self.solver = self._path.solver
+        if self._sr:
+            # fields by the split u = rho_s u_1 + u_s (primary.py); the
+            # geometric primary and A(1) u_1 are formed once here
+            self._path.set_primary(
+                unit_primary(mesh, survey, self.kys),
+                (L @ np.ones(self.nC)).reshape(self.nky, self.nnzA),
+                source_cells(mesh, survey), self._rho_p)
         self.sidx = torch.as_tensor(ops.sidx, device=self.device)
         self.iD = torch.arange(self.nD, device=self.device)
         self.wq = torch.as_tensor(self.wq_np, dtype=torch.float64,
@@ -217,6 +223,7 @@ class TorchDC2D:
         (dctorch/simulation2d.py:439-518): the adjoint right-hand sides are the
         columns of Pd^T, solved `block` data at a time on the same factors.
         Returned outside the autograd graph on m's device and dtype."""
+        self._plain_only("Jmatrix")
         block = max(1, min(int(block), self.nD, self._path.width))
         with torch.no_grad():
             m_full = self._model_to_full(m)
@@ -231,8 +238,16 @@ class TorchDC2D:
     def linearize(self, m, store_fields=None, fields_max_gib=2.0):
         """The forward frozen at m: one factorization, the fields kept, and
         J v / J^T v as one batched solve each (see `Linearization2D`)."""
+        self._plain_only("linearize")
         return Linearization2D(self, m, store_fields=store_fields,
                                fields_max_gib=fields_max_gib)
+
+    def _plain_only(self, what):
+        if self._sr:
+            raise NotImplementedError(
+                f"{what} is built for the plain formulation only (as in "
+                "dctorch/simulation2d.py:471-476, 572-577); with singularity "
+                "removal use dpred, misfit, misfit_and_grad or Jtvec")
 
     def Jvec(self, m, v):
         """J v without forming J (dctorch/simulation2d.py:526-529)."""

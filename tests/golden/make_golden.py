@@ -29,6 +29,11 @@ path in float64:
       IP data and the misfit gradient with respect to eta.  The IP
       constructors build their DC engine themselves (which needs SimPEG);
       here that name is pointed at the stub engines above while they run.
+  sr_tiny.npz     : TorchDC2D with singularity removal
+      (dctorch/simulation2d.py:306-333 with dctorch/singularity.py) on the
+      tiny 2-D problem, background from the model and fixed: dpred, misfit,
+      its gradient, Jtvec, chunked Jtvec and misfit_and_grad.  The primary
+      is kept in host memory (no CUDA here: pin_memory is skipped).
   dcip_tiny.npz   : the joint non-linear DC + IP engine (dctorch/dcip2d.py
       TorchDCIP2D) on the tiny 2-D problem for both DC states: the DC and
       IP data of a stacked (log-rho, logit-eta) model and the gradient of
@@ -270,6 +275,7 @@ def main():
     np.savez_compressed(os.path.join(out, "ip_tiny.npz"),
                         **ip_fixture(a.reference, S, Q, S2, S3))
     np.savez_compressed(os.path.join(out, "dcip_tiny.npz"), **dcip_fixture(S, Q, S2))
+    np.savez_compressed(os.path.join(out, "sr_tiny.npz"), **sr_fixture(Q, S2))
 
 
 def mark_chargeability(survey):
@@ -325,6 +331,28 @@ def ip_fixture(root, S, Q, S2, S3):
                     f"{tag}_grad": et.grad.numpy()})
         print("ip", tag, "nD", d.size, "chargeability data",
               int((ip._scale.numpy() != 1.0).sum()))
+    return rec
+
+
+def sr_fixture(Q, S2):
+    mesh, survey, m = syn.tiny_2d()
+    ops = nodal_operators(mesh, survey)
+    rmin, rmax = electrode_distance_range(survey)
+    kys, wq, _ = Q.k0_quadrature(rmin, rmax, 7)
+    rec = dict(kys=kys, wq=wq, m=m)
+    pin = torch.Tensor.pin_memory
+    torch.Tensor.pin_memory = lambda self, *a, **k: self
+    try:
+        for tag, rho_p in (("model", None), ("fixed", 50.0)):
+            eng, _ = engine_2d(S2, ops, kys, wq)
+            eng._sr, eng._rho_p, eng._mesh, eng._survey = True, rho_p, mesh, survey
+            dobs, w, v = data_vectors(eng, m, 51)
+            res = run_engine(eng, m, dobs, w, v, True)
+            rec.update({f"{tag}_{k}": x for k, x in
+                        dict(dobs=dobs, w=w, v=v, **res).items()})
+            print("sr", tag, "nD", dobs.size)
+    finally:
+        torch.Tensor.pin_memory = pin
     return rec
 
 

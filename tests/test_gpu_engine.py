@@ -155,3 +155,32 @@ def test_adjoint_survives_a_clobbered_factorization(cuda):
         eng.dpred(torch.tensor(g["m"] + 0.3, device=cuda))
     phi.backward()
     assert rel(mt.grad.cpu().numpy(), g["grad"]) < 1e-9
+
+
+@pytest.mark.parametrize("tag,rho_p", [("model", None), ("fixed", 50.0)])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_dc2d_singularity_removal_matches_reference(cuda, tag, rho_p, dtype):
+    """TorchDC2D(singularity_removal=True) against the reference's own
+    (golden sr_tiny: dctorch/simulation2d.py:306-333 with
+    dctorch/singularity.py), the primary's background from the model or
+    fixed; the Jacobian products of the plain formulation refuse, as there."""
+    g = golden("sr_tiny")
+    mesh, survey, _ = syn.tiny_2d()
+    eng = TorchDC2D(mesh, survey, nky=7, device=cuda, dtype=dtype,
+                    quadrature=(g["kys"], g["wq"]), singularity_removal=True,
+                    rho_primary=rho_p)
+    d, phi, grad, jt = _run(eng, g["m"], g[f"{tag}_dobs"], g[f"{tag}_w"],
+                            g[f"{tag}_v"], cuda)
+    tol_d, tol_g = (1e-10, 1e-9) if dtype == torch.float64 else (1e-6, 1e-5)
+    assert rel(d, g[f"{tag}_dpred"]) < tol_d
+    assert abs(phi - g[f"{tag}_phi"]) <= tol_g * abs(g[f"{tag}_phi"])
+    assert rel(grad, g[f"{tag}_grad"]) < tol_g
+    assert rel(jt, g[f"{tag}_jtvec"]) < tol_g
+    f, gm = eng.misfit_and_grad(torch.tensor(g["m"], device=cuda),
+                                torch.tensor(g[f"{tag}_dobs"], device=cuda),
+                                torch.tensor(g[f"{tag}_w"], device=cuda))
+    assert abs(f - g[f"{tag}_mag_phi"]) <= tol_g * abs(g[f"{tag}_mag_phi"])
+    assert rel(gm.cpu().numpy(), g[f"{tag}_mag_grad"]) < tol_g
+    with pytest.raises(NotImplementedError):
+        eng.Jmatrix(torch.tensor(g["m"], device=cuda))
+    eng.check()
