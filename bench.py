@@ -20,8 +20,11 @@ instance of the workload (independent replicas: the path has no exchange
 step at one survey per GPU); the time is the max over ranks.
 
 `--impl reference` times the reference algorithm on the host cores (the CPU
-oracle, a float64 SuperLU restatement of the reference's CPU path) on a
-bounded sample of the workload, rank 0 only.
+oracle, a float64 SuperLU restatement of the reference's CPU path), rank 0
+only: the whole eval+grad per step on dc2d_small, an exactly scaled sample
+of the same workload on dc2d_large (see ReferenceCpu); on the 3-D workloads
+one eval+grad takes ~30 minutes on the CPU, and the arm prints an
+`unavailable` line with the measured figures instead.
 """
 from __future__ import annotations
 
@@ -40,40 +43,60 @@ sys.path.insert(0, ROOT)
 
 METRIC = "eval+grad ms, FP32+IR vs plain FP64 on same B200, at dpred rel-err ≤1e-6"
 
+# l2: how the timed steps avoid reading a warm L2 (126 MB) -- inputs larger
+# than L2, or an L2 flush (a 512 MB write) between timed steps
 WORKLOADS = {
     "dc3d": dict(desc="3-D DC, TensorMesh 64x64x32 core @5 m + 8 padding/face "
                       "(x1.3), 10x10 surface grid, 200 pole-dipole sources, "
-                      "~30 receivers each"),
+                      "~30 receivers each",
+                 l2="inputs larger than L2 (float32 fronts 3.8 GB, fields 0.43 GB)",
+                 flush=False),
     "dc2d_large": dict(desc="2.5-D DC, TensorMesh 400x120 core @1 m + padding "
-                            "(x1.3), 96 electrodes, dipole-dipole + Wenner, nky 12"),
+                            "(x1.3), 96 electrodes, dipole-dipole + Wenner, nky 12",
+                       l2="inputs larger than L2 (float32 fronts 0.56 GB, fields 1.0 GB)",
+                       flush=False),
     "dc2d_small": dict(desc="2.5-D DC, TensorMesh 100x50 core @2.5 m + 10 padding "
-                            "(x1.3), 21 electrodes, dipole-dipole n=1..6, nky 11"),
+                            "(x1.3), 21 electrodes, dipole-dipole n=1..6, nky 11",
+                       l2="L2 flushed between timed steps (working set ~0.1 GB)",
+                       flush=True),
     # a reduced 3-D case for profiler captures (a few GB on the device)
     "dc3d_mid": dict(desc="3-D DC, TensorMesh 40x40x20 core @8 m + 6 padding/face "
-                          "(x1.3), same 200 sources and 6,000 data"),
+                          "(x1.3), same 200 sources and 6,000 data",
+                     l2="inputs larger than L2 (float32 fronts 0.62 GB)",
+                     flush=False),
 }
-# bounded CPU sample: the same workload family on a coarser grid
-CPU_SAMPLE = {
-    "dc3d": dict(kw=dict(ncore=(24, 24, 12), dx=13.0, npad=4),
-                 desc="3-D workload family coarsened: 24x24x12 core cells of "
-                      "13 m + 4 padding/face (18,513 nodes), same 200 sources "
-                      "and 6,000 data; one full eval+grad per step"),
-    "dc2d_large": dict(kw={}, desc="the full 2.5-D workload"),
-    "dc2d_small": dict(kw={}, desc="the full 2.5-D workload"),
-    "dc3d_mid": dict(kw=dict(ncore=(24, 24, 12), dx=13.0, npad=4),
-                     desc="coarsened as for dc3d"),
-}
+# The reference's CPU path (float64 SuperLU, scipy splu with its default
+# COLAMD ordering, single-threaded; dctorch/solver.py:314-374) cannot run
+# every workload inside a bench run.  Measured in the build container (one
+# core): the 269,001-node 3-D system takes 951.6 s to factor (nnz(L) =
+# nnz(U) = 4.46e8) and 23.8 s per 10 right-hand sides to solve, so one
+# eval+grad with 200 sources (factor + 2 x 200 right-hand sides) is ~1,900 s;
+# the 75,843-node 3-D case did not finish its factorization in 7 minutes.
+# The 2.5-D workloads factor in well under a second per wavenumber but solve
+# slowly (56,525 nodes: 39 s per wavenumber for 186 right-hand sides).
+REFERENCE_3D_UNAVAILABLE = (
+    "the reference's CPU path (float64 SuperLU, COLAMD, single-threaded) takes "
+    "~1,900 s per eval+grad on this 3-D workload (factorization of the 269,001-"
+    "node system measured at 951.6 s, solves at 23.8 s per 10 right-hand sides, "
+    "200 sources forward + 200 adjoint), so warm-up + timed steps cannot finish "
+    "in a bench run; no smaller grid stands in for it")
 
 
-def build_case(name, seed, sample=False):
+def build_case(name, seed):
     from simpeg_dc_torch_b200 import synthetic as syn
-    if name in ("dc3d", "dc3d_mid"):
-        kw = CPU_SAMPLE[name]["kw"] if sample else (
-            {} if name == "dc3d" else dict(ncore=(40, 40, 20), dx=8.0, npad=6))
-        return syn.dc3d(seed=seed, **kw)
+    if name == "dc3d":
+        return syn.dc3d(seed=seed)
+    if name == "dc3d_mid":
+        return syn.dc3d(seed=seed, ncore=(40, 40, 20), dx=8.0, npad=6)
     if name == "dc2d_large":
         return syn.dc2d_large(seed=seed)
     return syn.dc2d_small(seed=seed)
+
+
+def workload_config(name):
+    """The workload as both arms name it (identical dicts)."""
+    return {"workload": name, "description": WORKLOADS[name]["desc"],
+            "l2": WORKLOADS[name]["l2"]}
 
 
 def make_engine(name, mesh, survey, device, dtype):
@@ -145,7 +168,6 @@ class ClockSampler:
 
 # -------------------------------------------------------------- reference
 def oracle_ops(name, mesh, survey):
-    from oracle import dc_oracle as O  # noqa: F401
     from simpeg_dc_torch_b200.operators import nodal_operators
     from simpeg_dc_torch_b200.quadrature import (electrode_distance_range,
                                                  k0_quadrature)
@@ -163,53 +185,117 @@ def oracle_ops(name, mesh, survey):
     return op
 
 
-def cpu_eval_grad_timer(name, seed=0):
-    """Returns (run_once, sample description): one oracle eval+grad."""
-    from oracle import dc_oracle as O
-    from simpeg_dc_torch_b200 import synthetic as syn
-    mesh, survey, m = build_case(name, seed, sample=True)
-    op = oracle_ops(name, mesh, survey)
-    three_d = name.startswith("dc3d")
-    d = O.dpred_3d(op, m) if three_d else O.dpred_2d(op, m)
-    dobs, w = syn.observed(d, np.random.default_rng(seed + 1))
+class ReferenceCpu:
+    """The reference's CPU eval+grad (the oracle's SuperLU restatement of
+    dctorch/solver.py:314-374 with the engines' chain) on a 2.5-D workload.
 
-    def once():
+    dc2d_small: one full eval+grad per step.  dc2d_large: each step is a
+    bounded sample of the same workload -- the factorization of one of its
+    wavenumber systems (cycling through them) and the forward and adjoint
+    solves of all source columns on it, as the reference's batch solver
+    does per system -- scaled exactly to one eval+grad: the wavenumber
+    systems are independent, so eval+grad = nky (t_factor + t_solves) +
+    t_rest, with the projection / contraction rest timed once on the full
+    problem.  `cols` < the source count solves that many columns and scales
+    the solve time linearly (SuperLU solves column by column)."""
+
+    def __init__(self, name, seed=0, cols=None):
+        from oracle import dc_oracle as O
+        from simpeg_dc_torch_b200 import synthetic as syn
+        self.name, self.O = name, O
+        mesh, survey, m = build_case(name, seed)
+        self.op = op = oracle_ops(name, mesh, survey)
+        self.m = m
+        self.nky = len(op["wq"])
+        self.nS = op["Q"].shape[1]
+        self.cols = self.nS if cols is None else min(int(cols), self.nS)
+        self.vals = O.vals_2d(op["Lstack"], m, self.nky)
+        self.step_i = 0
+        if name == "dc2d_small":
+            d = O.dpred_2d(op, m)
+            self.dobs, self.w = syn.observed(d, np.random.default_rng(seed + 1))
+            self.desc = "the full workload: one eval+grad per step"
+            return
+        # the rest of the chain around the solves, on the full problem:
+        # quadrature sum + projection, adjoint scatter, contraction, L^T
+        rng = np.random.default_rng(seed + 1)
+        U = rng.standard_normal((self.nky, op["nN"], self.nS))
         t = time.perf_counter()
-        if three_d:
-            O.misfit_grad_3d(op, m, dobs, w)
-        else:
-            O.misfit_grad_2d(op, m, dobs, w)
-        return 1e3 * (time.perf_counter() - t)
-    return once, CPU_SAMPLE[name]["desc"]
+        Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
+        PU = op["Pd"] @ Ubar
+        d = PU[np.arange(PU.shape[0]), op["sidx"]]
+        G = np.zeros((op["Pd"].shape[0], self.nS))
+        G[np.arange(G.shape[0]), op["sidx"]] = d
+        GU = op["Pd"].T @ G
+        r = O.row_of(op["crow"])
+        gv = np.empty((self.nky, len(op["col"])))
+        for k in range(self.nky):
+            gv[k] = -op["wq"][k] * np.einsum("es,es->e", U[k][r], U[k][op["col"]])
+        _ = op["Lstack"].T @ gv.reshape(-1) + GU.sum()
+        self.t_rest = 1e3 * (time.perf_counter() - t)
+        self.desc = (f"each step: SuperLU factorization of one of the "
+                     f"{self.nky} wavenumber systems and forward + adjoint "
+                     f"solves of {self.cols} of its {self.nS} source columns, "
+                     f"scaled exactly to one eval+grad ({self.nky} systems, "
+                     f"{self.nS} columns each way) plus the projection / "
+                     f"contraction rest timed once ({self.t_rest:.0f} ms)")
+
+    def step(self):
+        O, op = self.O, self.op
+        if self.name == "dc2d_small":
+            t = time.perf_counter()
+            O.misfit_grad_2d(op, self.m, self.dobs, self.w)
+            return 1e3 * (time.perf_counter() - t)
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spla
+        k = self.step_i % self.nky
+        c0 = (self.step_i * self.cols) % self.nS
+        self.step_i += 1
+        cols = np.arange(c0, c0 + self.cols) % self.nS
+        t = time.perf_counter()
+        lu = spla.splu(sp.csr_matrix((self.vals[k], op["col"], op["crow"]),
+                                     shape=(op["nN"], op["nN"])).tocsc())
+        t_f = time.perf_counter() - t
+        B = np.ascontiguousarray(op["Q"][:, cols])
+        t = time.perf_counter()
+        x = lu.solve(B)
+        lu.solve(np.ascontiguousarray(x[::-1]))      # the adjoint solve
+        t_s = time.perf_counter() - t
+        return 1e3 * self.nky * (t_f + t_s * self.nS / self.cols) + self.t_rest
+
+
+def reference_line(args, ms, desc, cores):
+    return {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(args.workload),
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores,
+                         "kind": "port", "sample": desc,
+                         "note": "float64 SuperLU (scipy splu, COLAMD, "
+                                 "single-threaded) restatement of the "
+                                 "reference's CPU path"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    once, desc = cpu_eval_grad_timer(args.workload)
+    if args.workload.startswith("dc3d"):
+        print(json.dumps({"impl": "reference", "metric": METRIC,
+                          "config": workload_config(args.workload),
+                          "unavailable": REFERENCE_3D_UNAVAILABLE}), flush=True)
+        return 0
+    ref = ReferenceCpu(args.workload)
     for _ in range(args.warmup):
-        once()
-    ts = [once() for _ in range(args.steps)]
+        ref.step()
+    ts = [ref.step() for _ in range(args.steps)]
     ms = float(np.mean(ts))
-    cores = os.cpu_count()
-    line = {
-        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload,
-                   "description": WORKLOADS[args.workload]["desc"],
-                   "sample": desc},
-        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores,
-                         "kind": "port", "sample": desc,
-                         "note": "float64 SuperLU (scipy splu, single-threaded "
-                                 "factorization) restatement of the reference's "
-                                 "CPU path"},
-        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+    print(json.dumps(reference_line(args, ms, ref.desc, 1)), flush=True)
     return 0
 
 
@@ -234,8 +320,11 @@ def count_launches(eng):
     if code == 0:
         solve = 1 + passes                       # rhs copy + substitution
     else:
+        # conversion, first solve and update, then per correction the
+        # residual, the solve, the update and the stopping decision (the
+        # launches of corrections not needed still run, and return at entry)
         ir = eng.solver.refine
-        solve = 1 + (1 + ir) * (passes + 1) + ir  # + updates and residuals
+        solve = 2 + passes + ir * (passes + 3)
     # sigma/values (2), source scatter, projection, adjoint scatter,
     # gather-contract, values vjp
     return 7 + factor + 2 * solve
@@ -256,6 +345,29 @@ def max_over_ranks(x, world, device):
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def cpu_baseline_leg(name):
+    """The reference's CPU path timed on the host cores beside the GPU line:
+    a bounded run of `ReferenceCpu` steps (2.5-D workloads, ~20 s), or, for
+    the 3-D workloads, the reason it cannot run with the full-size record."""
+    if name.startswith("dc3d"):
+        out = {"value": None, "unit": "ms", "cores": 1, "kind": "port",
+               "sample": "none", "unavailable": REFERENCE_3D_UNAVAILABLE}
+        if name == "dc3d":
+            # 951.6 s factorization + 2 x 200 right-hand sides at 2.38 s each
+            out["recorded_full_size_estimate_ms"] = 1e3 * (951.6 + 2 * 200 * 2.38)
+        return out
+    ref = ReferenceCpu(name)
+    ref.step()
+    t0 = time.perf_counter()
+    ts = []
+    while len(ts) < 3 or (len(ts) < 10 and time.perf_counter() - t0 < 20):
+        ts.append(ref.step())
+    return {"value": float(np.mean(ts)), "unit": "ms", "cores": 1,
+            "kind": "port", "sample": ref.desc,
+            "note": "float64 SuperLU (scipy splu, COLAMD, single-threaded) "
+                    "restatement of the reference's CPU path"}
 
 
 def main():
@@ -310,9 +422,15 @@ def main():
         phi.backward()
         return phi.detach(), x.grad
 
-    # accuracy of the float32 + refinement path against float64
+    # accuracy of the float32 + refinement path against float64, and the
+    # refinement record of the forward and adjoint solves of that step
     phi64, g64 = eval_grad(e64, m)
+    e32._path.record_refinement = True
     phi32, g32 = eval_grad(e32, m)
+    e32._path.record_refinement = False
+    refinement = {k: {"corrections": v["iters"], "converged": v["converged"],
+                      "est_error": v["est_error"], "rho": v["rho"]}
+                  for k, v in e32._path.last_refinement.items()}
     with torch.no_grad():
         d32 = e32.dpred(m)
     e32.check()
@@ -321,33 +439,53 @@ def main():
            "grad_rel": float(torch.linalg.norm(g32 - g64) / torch.linalg.norm(g64)),
            "phi_rel": float(abs(phi32 - phi64) / abs(phi64))}
 
-    def timed(eng, steps, warmup, sampler=None, tag=None):
+    # working sets below L2: a 512 MB write between timed steps, outside
+    # the timed events
+    flush_buf = (torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+                 if WORKLOADS[args.workload]["flush"] else None)
+
+    def timed_loop(step, steps, warmup, sampler=None, tag=None):
         for _ in range(warmup):
-            eval_grad(eng, m)
+            step()
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
         if sampler:
             sampler.start()
         st = torch.cuda.current_stream()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
         if tag:   # NVTX range: lets a profiler select the timed launches
             torch.cuda.nvtx.range_push(tag)
-        a.record(st)
-        for _ in range(steps):
-            eval_grad(eng, m)
-        b.record(st)
+        pairs = []
+        if flush_buf is None:
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(steps):
+                step()
+            b.record(st)
+            pairs.append((a, b))
+        else:
+            for _ in range(steps):
+                flush_buf.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                step()
+                b.record(st)
+                pairs.append((a, b))
         if tag:
             torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
         barrier()
-        return rank_max(a.elapsed_time(b) / steps), clocks
+        ms = sum(a.elapsed_time(b) for a, b in pairs) / steps
+        return rank_max(ms), clocks
 
     sampler = ClockSampler(local)
-    ms32, clocks = timed(e32, args.steps, args.warmup, sampler, tag="timed_fp32")
-    ms64, _ = timed(e64, args.steps, args.warmup, tag="timed_fp64")
+    ms32, clocks = timed_loop(lambda: eval_grad(e32, m), args.steps, args.warmup,
+                              sampler, tag="timed_fp32")
+    ms64, _ = timed_loop(lambda: eval_grad(e64, m), args.steps, args.warmup,
+                         tag="timed_fp64")
 
     # end to end through the public API, host buffers in and out
     e2e = None
@@ -367,19 +505,7 @@ def main():
             g_h.copy_(md.grad, non_blocking=True)
             phi_h.copy_(phi.detach(), non_blocking=True)
 
-        for _ in range(args.warmup):
-            e2e_step()
-        torch.cuda.synchronize()
-        barrier()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(args.steps):
-            e2e_step()
-        b.record()
-        torch.cuda.synchronize()
-        barrier()
-        e2e_ms = rank_max(a.elapsed_time(b) / args.steps)
+        e2e_ms, _ = timed_loop(e2e_step, args.steps, args.warmup)
         e2e = {"value": e2e_ms, "unit": "ms",
                "h2d_bytes_per_step": (m_h.numel() + dobs_h.numel()
                                       + w_h.numel()) * 8,
@@ -396,17 +522,16 @@ def main():
     tot = sum(v[0] for v in prof.values())
     dom = max(prof, key=lambda k: prof[k][0])
     dms, dn, dfl, dby = prof[dom]
-    import json as _j
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
-        peaks = _j.load(open(pk))
+        peaks = json.load(open(pk))
     hbm = peaks.get("hbm_gbs", 6650.0)
     tc = peaks.get("bf16_tflops", 1590.0)
     traffic = None
     tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tj):
-        traffic = _j.load(open(tj)).get(args.workload, {}).get(dom)
+        traffic = json.load(open(tj)).get(args.workload, {}).get(dom)
     if dom in TENSOR_KINDS:
         ach = dfl / (dms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
@@ -430,17 +555,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        once, desc = cpu_eval_grad_timer(args.workload)
-        once()
-        t0 = time.perf_counter()
-        ts = []
-        while len(ts) < 3 and time.perf_counter() - t0 < 20:
-            ts.append(once())
-        cpu = {"value": float(np.mean(ts)), "unit": "ms",
-               "cores": os.cpu_count(), "kind": "port", "sample": desc,
-               "note": "CPU oracle (float64 SuperLU restatement of the "
-                       "reference's CPU path); SuperLU factorization is "
-                       "single-threaded"}
+        cpu = cpu_baseline_leg(args.workload)
 
     sinfo = e32.solver.analysis()
     if rank == 0:
@@ -450,18 +565,15 @@ def main():
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 factor/solve + f64 refinement, f64 data/misfit",
             "data": "synthetic (seeded)",
-            "config": {"workload": args.workload,
-                       "description": WORKLOADS[args.workload]["desc"],
-                       "cells": int(e32.nC), "nodes": int(e32.nN),
-                       "sources": int(e32.nS), "data": int(e32.nD),
-                       "nsystems": int(e32.solver.nbatch),
-                       "nnz_L": int(sinfo["nnz_L"]),
-                       "factor_flops": float(sinfo["flops_factor"]),
-                       "l2": "inputs larger than L2 (float32 fronts "
-                             f"{4 * sinfo['front_total'] * e32.solver.nbatch / 1e9:.2f} GB)",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args.workload),
+            "problem": {"cells": int(e32.nC), "nodes": int(e32.nN),
+                        "sources": int(e32.nS), "data": int(e32.nD),
+                        "nsystems": int(e32.solver.nbatch),
+                        "nnz_L": int(sinfo["nnz_L"]),
+                        "factor_flops": float(sinfo["flops_factor"]),
+                        "parallelism": f"replicas x{world}"},
             "fp64_ms": ms64, "speedup_vs_fp64": ms64 / ms32,
-            "accuracy_vs_fp64": acc,
+            "accuracy_vs_fp64": acc, "refinement": refinement,
             "e2e": e2e, "gpu_launches": count_launches(e32),
             "roofline": roof,
             "kernel_ms": {k: v[0] / 2 for k, v in prof.items()},

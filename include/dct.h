@@ -97,7 +97,28 @@ int dct_symbolic_get_schedule(const dct_symbolic* sym, int32_t dtype,
 int dct_plan_create(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
                     int32_t dtype, int32_t device, dct_plan** out);
 void dct_plan_destroy(dct_plan* plan);
+/* Iterative refinement of float32 plans (no effect on float64 plans):
+ * at most `iterations` corrections (default 2, at most 64) after the first
+ * solve; each correction i adds c_i = A_32^{-1} (b - A x) with the residual
+ * formed in float64.  rho_i = max|c_i| / max|x_i| estimates the relative
+ * error of the previous iterate, so rho_i * min(1, rho_i / rho_{i-1})
+ * (rho_1^2 for the first) estimates that of x_i.  Refinement stops once that
+ * estimate is <= tol (default 1e-10); when the corrections stagnate
+ * (rho_i > rho_{i-1} / 2, or NaN) or the iterations run out above tol, the
+ * plan's status words record DCT_ERR_IR_NOT_CONVERGED (read by
+ * dct_check_status, `where` = -1).  The decision is taken on the device: the
+ * launches of corrections that are not needed return at entry and the host
+ * never waits.  Replaces the fixed precision of CuDSSSolver's float32 solves
+ * (dctorch/solver.py:122-135), which has no refinement. */
 int dct_plan_set_refinement(dct_plan* plan, int32_t iterations);
+int dct_plan_set_refinement_tolerance(dct_plan* plan, double tol);
+/* The refinement record of the plan's last float32 solve (synchronises the
+ * stream): corrections applied, whether the estimate reached the tolerance,
+ * the estimated relative error and rho_1 .. rho_iters (first min(capacity,
+ * iters, 16) of them). */
+int dct_plan_refinement_info(dct_plan* plan, void* stream, int32_t* iters,
+                             int32_t* converged, double* est_error, double* rho,
+                             int32_t capacity);
 /* device pointer to the plan's iperm (int32, n): user row -> permuted row */
 int dct_plan_iperm(const dct_plan* plan, const int32_t** d_iperm);
 /* bumped by every factorization (dctorch/solver.py:211-213, 221) */
@@ -247,16 +268,21 @@ int dct_values_vjp_multi(int64_t nC, int32_t nb, const int64_t* d_Lt_ptr,
 
 /* ---- allocation-free small solve -------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory (work inside a stream being captured into a CUDA graph, hosts whose
- * framework owns all device memory, loops that cannot take the device-wide
- * synchronisation of cudaMalloc/cudaFree): factors one SPD system given by
- * its CSR pattern and values (n <= 512; the lower triangle is read) and
- * solves k <= 64 right-hand sides, b and x row-major (n, k) float64 on the
- * current device.  Its only scratch is a fixed 2 MiB array in the library
- * (held by every GPU that loads the library until exit); sizes beyond the
- * limits return DCT_ERR_ARG.  The first call on a device looks up that
- * array's address and must come before any stream capture.  Calls share the
- * array, so calls that may overlap on the GPU race and must be ordered. */
+ * memory (hosts whose framework owns all device memory through its own pool,
+ * loops that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree): factors one SPD system given by its CSR pattern and
+ * values (n <= 512; the lower triangle is read) and solves k <= 64
+ * right-hand sides, b and x row-major (n, k) float64 on the current device.
+ * Its only scratch is a fixed 2 MiB array in the library (held by every GPU
+ * that loads the library until exit); sizes beyond the limits return
+ * DCT_ERR_ARG.  The first call on a device looks up that array's address and
+ * should come before any stream capture.  Calls share the array, so calls
+ * that may overlap on the GPU race and must be ordered.  The call does not
+ * wait for the GPU: a matrix that is not positive definite (a non-positive
+ * or NaN pivot) makes every entry of x NaN rather than returning a status.
+ * The pattern must be canonical (columns in [0, n), no duplicates: a
+ * duplicate overwrites instead of adding); out-of-range columns and
+ * decreasing row pointers are skipped. */
 int dct_solve_small_noalloc(int32_t n, const int32_t* d_crow,
                             const int32_t* d_col, const double* d_vals,
                             const double* d_b, int32_t k, double* d_x,

@@ -9,6 +9,11 @@ Pinned: `tests/golden/*.npz` hold outputs of the reference itself (its
 runtime, driven with the same operators); `tests/test_oracle.py` checks this
 module against them.
 
+Two exact float64 solvers stand behind it: `SuperLUBatch` (the reference's
+own CPU solver, scipy SuperLU) and `SlabCholeskyBatch`, a block-tridiagonal
+dense Cholesky over the grid slabs for the workloads at which SuperLU takes
+minutes per factorization (selected by an operator set's "slab" entry).
+
 Operators (names as in the reference engines):
   Lstack  : CSR (nky*nnzA, nC), values of A_k = rows k*nnzA .. (k+1)*nnzA
   crow,col: CSR pattern of A (nN+1,), (nnzA,)
@@ -50,6 +55,136 @@ class SuperLUBatch:
 
 def row_of(crow):
     return np.repeat(np.arange(len(crow) - 1), np.diff(crow))
+
+
+class SlabCholeskyBatch:
+    """Exact float64 solves of nbatch SPD systems on one grid pattern by a
+    block-tridiagonal dense Cholesky, for problems too large for SuperLU's
+    single-threaded factorization and column-by-column solves.  It computes
+    the same x = A^{-1} b as `SuperLUBatch` (dctorch/solver.py:314-374) to
+    rounding, by another direct method, which `tests/test_oracle.py` checks.
+
+    `slab[i]` is the grid slab of node i (its index along one mesh axis); the
+    nodal stencil couples only nodes of the same or adjacent slabs, so with
+    the nodes grouped slab by slab A is block tridiagonal:
+        L_ii L_ii^T = A_ii - L_i,i-1 L_i,i-1^T,
+        L_i+1,i     = A_i+1,i L_ii^{-T},
+    and the solves are blocked forward / backward substitutions over the
+    slabs (LAPACK potrf / trsm / gemm on dense blocks)."""
+
+    def __init__(self, crow, col, n, slab):
+        self.crow = np.asarray(crow)
+        self.col = np.asarray(col)
+        self.n = int(n)
+        slab = np.asarray(slab, dtype=np.int64)
+        if slab.shape != (self.n,):
+            raise ValueError("one slab index per node")
+        r = row_of(self.crow)
+        if np.abs(slab[r] - slab[self.col]).max(initial=0) > 1:
+            raise ValueError("the pattern couples nodes of non-adjacent slabs")
+        self.order = np.argsort(slab, kind="stable")
+        self.starts = np.searchsorted(slab[self.order],
+                                      np.arange(int(slab.max()) + 2))
+        self.fac = []
+
+    # BLAS threads of the dense block kernels: the blocks are small (one
+    # grid slab), and more threads than this only add synchronisation
+    BLAS_THREADS = 4
+
+    def _threads(self):
+        import os
+        from threadpoolctl import threadpool_limits
+        return threadpool_limits(limits=max(1, min(self.BLAS_THREADS,
+                                                   os.cpu_count() or 1)),
+                                 user_api="blas")
+
+    def factorize(self, vals):
+        with self._threads():
+            self._factorize(vals)
+
+    def _factorize(self, vals):
+        import scipy.linalg as sla
+        vals = np.atleast_2d(np.asarray(vals, float))
+        o, st = self.order, self.starts
+        self.fac = []
+        for v in vals:
+            A = sp.csr_matrix((v, self.col, self.crow), shape=(self.n, self.n))
+            A = A[o][:, o].tocsr()
+            diag, sub = [], []
+            prev = None
+            for i in range(len(st) - 1):
+                a, b = st[i], st[i + 1]
+                D = A[a:b, a:b].toarray()
+                if prev is not None:
+                    D -= prev @ prev.T
+                Lii = sla.cholesky(D, lower=True, check_finite=False)
+                diag.append(Lii)
+                if i + 2 < len(st):
+                    B = A[b:st[i + 2], a:b].toarray()
+                    prev = _flush_tiny(sla.solve_triangular(
+                        Lii, B.T, lower=True, check_finite=False).T)
+                    sub.append(prev)
+            self.fac.append((diag, sub))
+
+    def _solve_one(self, f, B):
+        import scipy.linalg as sla
+        diag, sub = f
+        st = self.starts
+        X = np.array(B[self.order], dtype=float)
+        ns = len(st) - 1
+        for i in range(ns):
+            a, b = st[i], st[i + 1]
+            rhs = X[a:b]
+            if i > 0:
+                rhs = rhs - sub[i - 1] @ X[st[i - 1]:a]
+            X[a:b] = _flush_tiny(sla.solve_triangular(diag[i], rhs, lower=True,
+                                                      check_finite=False))
+        for i in range(ns - 1, -1, -1):
+            a, b = st[i], st[i + 1]
+            rhs = X[a:b]
+            if i + 1 < ns:
+                rhs = rhs - sub[i].T @ X[b:st[i + 2]]
+            X[a:b] = _flush_tiny(sla.solve_triangular(diag[i], rhs, lower=True,
+                                                      trans="T", check_finite=False))
+        out = np.empty_like(X)
+        out[self.order] = X
+        return out
+
+    def solve(self, B):
+        """B: (n, k) shared, or (nbatch, n, k); returns (nbatch, n, k)."""
+        B = np.asarray(B, float)
+        with self._threads():
+            if B.ndim == 2:
+                return np.stack([self._solve_one(f, B) for f in self.fac])
+            return np.stack([self._solve_one(f, B[i]) for i, f in enumerate(self.fac)])
+
+
+def _flush_tiny(X):
+    """Entries below 1e-100 of the block's largest set to zero: the coupling
+    blocks decay geometrically away from the slab interface, and products
+    of such entries would otherwise fall into subnormal floating point,
+    which slows the dense kernels by orders of magnitude.  The perturbation
+    is 1e-100 relative, far below float64 rounding."""
+    big = np.abs(X).max(initial=0.0)
+    if big > 0.0:
+        X[np.abs(X) < 1e-100 * big] = 0.0
+    return X
+
+
+def grid_slabs(node_grid):
+    """Slab index of every node for `SlabCholeskyBatch`: its grid index along
+    the axis with the most nodes (the smallest dense blocks)."""
+    g = np.asarray(node_grid)
+    ax = int(np.argmax(g.max(axis=0)))
+    return g[:, ax]
+
+
+def _batch_solver(op):
+    """The exact solver of the operator set: SuperLU (the reference's CPU
+    solver) unless op carries grid slabs for the block solver."""
+    if op.get("slab") is not None:
+        return SlabCholeskyBatch(op["crow"], op["col"], op["nN"], op["slab"])
+    return SuperLUBatch(op["crow"], op["col"], op["nN"])
 
 
 def sparse_solve_vjp(crow, col, vals, b, gx):
@@ -96,7 +231,7 @@ def dpred_2d(op, m, return_fields=False):
     d = (Pd Ubar)[i, sidx[i]]."""
     nky = len(op["wq"])
     VALS = vals_2d(op["Lstack"], m, nky)
-    slv = SuperLUBatch(op["crow"], op["col"], op["nN"])
+    slv = _batch_solver(op)
     slv.factorize(VALS)
     U = slv.solve(op["Q"])
     Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
@@ -192,7 +327,7 @@ def diag_jtdj_2d(op, m, dw):
 def dpred_3d(op, m, return_fields=False):
     """simulation3d.py:197-207: VALS = L3 exp(-m); U = A^{-1} q; d = (Pd U)[i, sidx]."""
     vals = op["L3"] @ sigma_of(m)
-    slv = SuperLUBatch(op["crow"], op["col"], op["nN"])
+    slv = _batch_solver(op)
     slv.factorize(vals[None])
     U = slv.solve(op["Q"])[0]
     PU = op["Pd"] @ U
@@ -335,7 +470,7 @@ def dpred_2d_sr(op, m, u1, return_fields=False):
     VALS = vals_2d(op["Lstack"], m, nky)
     ONES = (op["Lstack"] @ np.ones(op["Lstack"].shape[1])).reshape(nky, -1)
     n = op["nN"]
-    slv = SuperLUBatch(op["crow"], op["col"], n)
+    slv = _batch_solver(op)
     slv.factorize(VALS)
     B = np.stack([sp.csr_matrix((ONES[k], op["col"], op["crow"]), shape=(n, n)) @ u1[k]
                   for k in range(nky)])

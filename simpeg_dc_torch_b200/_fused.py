@@ -47,7 +47,8 @@ class FusedPath:
     """
 
     def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
-                 coords=None, refine=None, n_rhs=None, refine_fields=None):
+                 coords=None, refine=None, n_rhs=None, refine_fields=None,
+                 refine_tol=None):
         self.device = device
         nN = crow.size - 1
         self.nN, self.nnzA = nN, col.size
@@ -60,14 +61,19 @@ class FusedPath:
         self._pri = None      # singularity-removal split (set_primary)
         self.solver = DCTBatchSolver(crow, col, nN, self.width, self.nbatch,
                                      device=device, dtype=dt, coords=coords,
-                                     refine=refine)
+                                     refine=refine, refine_tol=refine_tol)
         plan = self.solver.plan
         self._plan = plan
-        # float32 plans: refinement iterations of the forward and of the
-        # adjoint fields.  One iteration brings the data to ~1e-8, but the
-        # gradient contracts both fields at every node and needs two each
-        # (measured on the 3-D workload: 3e-3 with one, 3e-6 with two).
+        # float32 plans: most refinement corrections of the forward and of
+        # the adjoint fields (each stops early at the plan's tolerance).  One
+        # correction brings the data to ~1e-8, but the gradient contracts
+        # both fields at every node and needs two each (measured on the 3-D
+        # workload: 3e-3 with one, 3e-6 with two).
         self.refine_adj = self.solver.refine
+        # with record_refinement set, every solve of the path synchronises
+        # and keeps its refinement record in last_refinement (diagnostics)
+        self.record_refinement = False
+        self.last_refinement = {}
         self.refine_fields = (self.refine_adj if refine_fields is None
                               else int(refine_fields))
         self._iperm_ptr = plan.d_iperm
@@ -157,10 +163,16 @@ class FusedPath:
                                   self._st())
         return x
 
+    def _record(self, what):
+        if self.record_refinement and self.solver.dtype == torch.float32:
+            self.last_refinement[what] = self.solver.refinement_info()
+
     def fields(self):
         """U = A^{-1} Q, permuted (nbatch, nN, nS)."""
         self._plan.set_refinement(self.refine_fields)
-        return self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
+        U = self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
+        self._record("fields")
+        return U
 
     # ------------------------------------------------ singularity removal
     def set_primary(self, u1, vals_one, src_cell, rho_fixed=None):
@@ -203,6 +215,7 @@ class FusedPath:
         self._plan.set_refinement(self.refine_fields)
         Us = torch.empty_like(rhs)
         self._plan.solve_permuted(rhs.data_ptr(), 1, self.nS, Us.data_ptr(), self._st())
+        self._record("fields")
         return Xs + Us
 
     def project(self, U):
@@ -236,6 +249,7 @@ class FusedPath:
         R = self._scatter(self._adj, g, self.nS)
         self._plan.set_refinement(self.refine_adj)
         Y = self._solve_perm(R, self.nS)
+        self._record("adjoint")
         gv = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
                          device=self.device)
         nat.check(nat.lib().dct_gather_contract(

@@ -65,6 +65,10 @@ _SIGS = {
     "dct_plan_create": (C.c_int, [_p, _i32, _i32, _i32, _i32, C.POINTER(_p)]),
     "dct_plan_destroy": (None, [_p]),
     "dct_plan_set_refinement": (C.c_int, [_p, _i32]),
+    "dct_plan_set_refinement_tolerance": (C.c_int, [_p, C.c_double]),
+    "dct_plan_refinement_info": (C.c_int, [_p, _p, _pi32, _pi32,
+                                           C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), _i32]),
     "dct_plan_iperm": (C.c_int, [_p, C.POINTER(_p)]),
     "dct_plan_stamp": (_i64, [_p]),
     "dct_factorize": (C.c_int, [_p, _p, _i32, _i64, _p]),
@@ -216,6 +220,21 @@ class Plan:
     def set_refinement(self, iters):
         check(lib().dct_plan_set_refinement(self._h, int(iters)),
               "dct_plan_set_refinement")
+
+    def set_refinement_tolerance(self, tol):
+        check(lib().dct_plan_set_refinement_tolerance(self._h, float(tol)),
+              "dct_plan_set_refinement_tolerance")
+
+    def refinement_info(self, stream):
+        """(corrections, converged, estimated error, [rho_1 ..]) of the last
+        float32 solve (synchronises the stream)."""
+        it, conv = C.c_int32(0), C.c_int32(0)
+        est = C.c_double(0.0)
+        rho = (C.c_double * 16)()
+        check(lib().dct_plan_refinement_info(self._h, stream, C.byref(it),
+                                             C.byref(conv), C.byref(est), rho, 16),
+              "dct_plan_refinement_info")
+        return it.value, bool(conv.value), est.value, list(rho[:min(it.value, 16)])
 
     def stamp(self):
         return int(lib().dct_plan_stamp(self._h))

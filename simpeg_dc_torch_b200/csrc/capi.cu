@@ -781,16 +781,46 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
   P->status = static_cast<int*>(p);
   if ((rc = alloc(P, 16, &p, "residual"))) return bail(rc);
   P->resid_bits = static_cast<unsigned long long*>(p);
+  if ((rc = alloc(P, sizeof(dct::IrState), &p, "refinement state"))) return bail(rc);
+  P->ir = static_cast<dct::IrState*>(p);
   if (cudaMemset(P->status, 0, 64) != cudaSuccess ||
-      cudaMemset(P->resid_bits, 0, 16) != cudaSuccess)
+      cudaMemset(P->resid_bits, 0, 16) != cudaSuccess ||
+      cudaMemset(P->ir, 0, sizeof(dct::IrState)) != cudaSuccess)
     return bail(fail(DCT_ERR_CUDA, "cudaMemset"));
   *out = P;
   return DCT_OK;
 }
 
 int dct_plan_set_refinement(dct_plan* P, int32_t iterations) {
-  if (!P || iterations < 0) return fail(DCT_ERR_ARG, "bad arguments");
+  if (!P || iterations < 0 || iterations > 64) return fail(DCT_ERR_ARG, "bad arguments");
   P->ir_iters = iterations;
+  return DCT_OK;
+}
+
+int dct_plan_set_refinement_tolerance(dct_plan* P, double tol) {
+  if (!P || !(tol >= 0.0)) return fail(DCT_ERR_ARG, "bad arguments");
+  P->ir_tol = tol;
+  return DCT_OK;
+}
+
+int dct_plan_refinement_info(dct_plan* P, void* stream, int32_t* iters,
+                             int32_t* converged, double* est_error, double* rho,
+                             int32_t capacity) {
+  if (!P || capacity < 0) return fail(DCT_ERR_ARG, "bad arguments");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  dct::IrState h{};
+  if (P->ir != nullptr) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DCT_CUDA(cudaMemcpyAsync(&h, P->ir, sizeof(h), cudaMemcpyDeviceToHost, st),
+             "refinement state read");
+    DCT_CUDA(cudaStreamSynchronize(st), "stream synchronize");
+  }
+  if (iters) *iters = h.iters;
+  if (converged) *converged = h.converged;
+  if (est_error) *est_error = h.est;
+  if (rho)
+    for (int i = 0; i < capacity && i < h.iters && i < dct::kIrHistory; ++i) rho[i] = h.rho[i];
   return DCT_OK;
 }
 
@@ -831,16 +861,21 @@ int solve_refined(dct_plan* P, const double* bp, int64_t bstride, int k,
   const int n = P->sym.n;
   const int64_t per = int64_t(n) * k;
   DCT_CUDA(cudaMemsetAsync(P->resid_bits, 0, 16, st), "memset");
+  DCT_CUDA(cudaMemsetAsync(P->ir, 0, sizeof(dct::IrState), st), "memset");
   DCT_CUDA(dct::launch_convert_any(bp, DCT_F64, bstride, per, P->nbatch, P->bufA,
                                    DCT_F32, st),
            "rhs conversion");
   DCT_CUDA(dct::run_solve_f32(P, k, st), "solve launch");
   DCT_CUDA(dct::launch_ir_update(P, xp, k, 1, st), "refinement update");
+  // corrections until the estimated error is below the tolerance, the
+  // iterations stagnate or ir_iters are spent; the decision is taken on the
+  // device (k_ir_decide), so the launches of the corrections that are not
+  // needed return at entry and the host never waits
   for (int it = 0; it < P->ir_iters; ++it) {
-    if (it + 1 == P->ir_iters) DCT_CUDA(cudaMemsetAsync(P->resid_bits, 0, 16, st), "memset");
     DCT_CUDA(dct::launch_residual(P, bp, bstride, xp, k, st), "residual");
     DCT_CUDA(dct::run_solve_f32(P, k, st), "solve launch");
     DCT_CUDA(dct::launch_ir_update(P, xp, k, 0, st), "refinement update");
+    DCT_CUDA(dct::launch_ir_decide(P, it + 1, st), "refinement decision");
   }
   return DCT_OK;
 }

@@ -10,6 +10,24 @@
 
 namespace dct {
 
+// Refinement state of one float32 solve, in device memory.  Iteration i adds
+// the correction c_i to x; its size rho_i = max|c_i| / max|x_i| estimates the
+// error of x_{i-1}, and rho_i * min(1, rho_i / rho_{i-1}) (rho_1^2 for the
+// first) that of x_i.  `done` is set once the estimate is below the plan's
+// tolerance, on stagnation (rho_i > rho_{i-1} / 2) or after the last allowed
+// iteration; kernels of later correction solves then return at entry.
+constexpr int kIrHistory = 16;
+struct IrState {
+  int done;                       // 1: no further corrections
+  int iters;                      // corrections applied after the first solve
+  int converged;                  // 1: estimate below the tolerance
+  int pad;
+  unsigned long long cmax, xmax;  // max|c|, max|x| of the last update (bits)
+  unsigned long long rmax, bmax;  // max|b - A x|, max|b| of the last residual
+  double est;                     // estimated relative error of x
+  double rho[kIrHistory];         // rho_1 .. rho_iters
+};
+
 // Device copy of the symbolic structure (plain pointers, passed by value).
 struct DevSym {
   const int32_t* sn_first;
@@ -194,7 +212,9 @@ struct dct_plan {
   unsigned long long* resid_bits = nullptr;  // device: max|r|, max|b|
   int factored = 0;
   int64_t stamp = 0;
-  int ir_iters = 2;                // refinement iterations of f32 plans
+  int ir_iters = 2;                // most refinement iterations of f32 plans
+  double ir_tol = 0.0;             // stop once the estimated error is below (0: fixed count)
+  dct::IrState* ir = nullptr;      // device: refinement state of the last solve
   int update_bpan = 1;             // panels per trailing-update block
   dct::Profiler prof;
 };
@@ -221,6 +241,9 @@ struct SolveArgs {
   const T* linv;
   const int64_t* linv_off;
   int64_t linv_stride;
+  // float32 plans: refinement state; a set `done` word makes every kernel of
+  // the remaining correction solves return at entry (null: never skip)
+  const int* skip;
 };
 // one launch of a tensor-core substitution kind (kFwdLinvTc .. kBwdLinvTc)
 cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g, int64_t count,
@@ -244,4 +267,6 @@ cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
                             const double* x, int k, cudaStream_t st);
 cudaError_t launch_ir_update(dct_plan* P, double* x, int k, int first,
                              cudaStream_t st);
+// decides after correction `iter` (1-based) whether to stop refining
+cudaError_t launch_ir_decide(dct_plan* P, int iter, cudaStream_t st);
 }  // namespace dct

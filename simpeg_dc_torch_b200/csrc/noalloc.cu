@@ -1,24 +1,30 @@
 // Allocation-free solve of one small SPD system (dct_solve_small_noalloc).
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// stream is being captured into a graph (cudaMalloc is not allowed there and
-// would end the capture), hosts whose framework owns every byte of device
-// memory through its own pool, and latency-bound loops that cannot afford the
-// device-wide synchronisation a cudaMalloc/cudaFree may cause.  For them this
-// entry point factors and solves a small system without any allocation: the
-// caller passes the CSR pattern and values, the right-hand sides and the
-// output, and the only scratch (the dense factor) lives in the file-scope
-// array below.  It holds kNoAllocMaxN^2 doubles (2 MiB) on every GPU that
-// loads the library, until the process exits.
+// Some callers of this library cannot allocate device memory: hosts whose
+// framework owns every byte of device memory through its own pool (a second
+// allocator would fight it for memory), and latency-bound loops that must not
+// take the device-wide synchronisation a cudaMalloc/cudaFree may cause.  For
+// them this entry point factors and solves a small system without any
+// allocation: the caller passes the CSR pattern and values, the right-hand
+// sides and the output, and the only scratch (the dense factor) lives in the
+// file-scope array below.  It holds kNoAllocMaxN^2 doubles (2 MiB) on every
+// GPU that loads the library, until the process exits.
 //
 // In host code `g_noalloc_factor` is a host-side stand-in, not a device
 // address; its device address is obtained once per device with
 // cudaGetSymbolAddress (with that device current) on the first call made on
-// that device, and cached.  That first call must therefore happen before any
+// that device, and cached.  That first call should therefore come before any
 // stream capture.  All calls share the one array and it keeps the contents of
 // the last call: each call clears the part it uses before writing it, and two
 // calls whose work overlaps on the GPU (different streams, no ordering) race
 // on it and must not be issued.
+//
+// The call returns without waiting for the GPU, so it cannot return a status
+// for a matrix that is not positive definite: a non-positive or NaN pivot
+// instead makes every entry of x NaN.  The CSR pattern must be canonical
+// (column indices in [0, n), no duplicates: a duplicate entry overwrites the
+// other instead of adding to it); entries with an out-of-range column, and
+// rows whose row pointers decrease, are skipped.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -45,7 +51,8 @@ __global__ void k_na_clear(double* __restrict__ S, int64_t count) {
     S[i] = 0.0;
 }
 
-// lower triangle of the CSR matrix into the dense column-major factor
+// lower triangle of the CSR matrix into the dense column-major factor;
+// entries whose column lies outside [0, i] are not stored
 __global__ void k_na_scatter(int n, const int32_t* __restrict__ crow,
                              const int32_t* __restrict__ col,
                              const double* __restrict__ vals,
@@ -54,14 +61,16 @@ __global__ void k_na_scatter(int n, const int32_t* __restrict__ crow,
        i += gridDim.x * blockDim.x)
     for (int e = crow[i]; e < crow[i + 1]; ++e) {
       const int j = col[e];
-      if (j <= i) S[i + int64_t(j) * n] = vals[e];
+      if (j >= 0 && j <= i) S[i + int64_t(j) * n] = vals[e];
     }
 }
 
 // Blocked right-looking Cholesky of the dense n x n lower triangle, one CTA.
 // Each 16-column panel is factored in shared memory, written back, and then
-// applied to the trailing lower triangle.  A non-positive pivot is replaced
-// by 1 so the call completes (the matrix must be SPD for a meaningful result).
+// applied to the trailing lower triangle.  A non-positive or NaN pivot
+// becomes NaN: it spreads through the rest of the factor and through both
+// substitutions (each of which reads every entry below the diagonal), so
+// every entry of x comes back NaN.
 __global__ void __launch_bounds__(kNaThreads) k_na_potrf(int n, double* __restrict__ S) {
   extern __shared__ double Ps[];   // (n - p0) x w panel, ld = n
   const int tid = threadIdx.x;
@@ -75,7 +84,7 @@ __global__ void __launch_bounds__(kNaThreads) k_na_potrf(int n, double* __restri
     __syncthreads();
     for (int c = 0; c < w; ++c) {
       double piv = Ps[c + c * m];
-      if (!(piv > 0.0)) piv = 1.0;
+      if (!(piv > 0.0)) piv = __longlong_as_double(0x7ff8000000000000ll);   // NaN
       const double d = sqrt(piv);
       __syncthreads();
       if (tid == 0) Ps[c + c * m] = d;

@@ -37,6 +37,11 @@ __device__ __forceinline__ void atomic_sub(T* p, T v) {
   atomicAdd(p, -v);
 }
 
+// a finished refinement: the remaining correction launches do nothing
+__device__ __forceinline__ bool ir_skip(const int* skip) {
+  return skip != nullptr && *reinterpret_cast<const volatile int*>(skip) != 0;
+}
+
 // resident CTAs per SM the CUDA-core substitution kernels are compiled for:
 // their shared memory admits 4 (float) / 2 (double); 3 caps float at 85
 // registers
@@ -90,6 +95,7 @@ __device__ __forceinline__ void load_dinv(T* S, const T* __restrict__ Di, int w,
 // one CTA: y = D^{-1} b (to B), then b[boundary rows] -= L_B y (atomics, A)
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_small(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
@@ -153,6 +159,7 @@ __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_small(Solv
 // accumulated over the panels before one atomic update per element.
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_bnd(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
@@ -202,6 +209,7 @@ __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_bnd(SolveA
 // large supernodes: y_s = L_ss^{-1} b_s, 64-row tile t0 per CTA (B <- A rows)
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_linv(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[a, k]
   T* S2 = S1 + kLD1 * kLD;                  // [k][j]: b[k, j]
@@ -244,6 +252,7 @@ __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_fwd_linv(Solve
 // large supernodes: x_s = L_ss^{-T} y_s, 64-row tile t0 per CTA (A <- B rows)
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_linv(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);   // [k][a], ld kLD1: Linv[k, a]
   T* S2 = S1 + kLD1 * kLD;                  // [k][j]: y[k, j]
@@ -307,6 +316,7 @@ __device__ void boundary_product(const T* F, int N, int ns, int c0, int w,
 // one CTA: y -= L_B^T x_B ; x = D^{-T} y (to A)
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_small(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
@@ -353,6 +363,7 @@ __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_small(Solv
 // large supernodes: y_p (B) -= L[boundary rows, panel p]^T x[boundary rows]
 template <typename T>
 __global__ void __launch_bounds__(kThreads, kSolveMinBlocks<T>) k_bwd_gemm(SolveArgs<T> g) {
+  if (ir_skip(g.skip)) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* S1 = reinterpret_cast<T*>(smem_raw);
   T* S2 = S1 + kLD1 * kLD;
@@ -437,13 +448,15 @@ __global__ void k_convert(const TI* __restrict__ src, int64_t sstride, int64_t c
 constexpr int kResidualRhs = DCT_RESIDUAL_RHS;
 
 // r = b - A x in float64 (permuted order), stored as float into the f32 work
-// buffer, with max|r| and max|b| folded into the plan's residual words.
+// buffer, with max|r| and max|b| folded into maxbits[0..1] (the refinement
+// state's rmax, bmax).
 
 __global__ void k_residual(DevSym S, const double* __restrict__ vals,
                            int64_t vals_stride, const double* __restrict__ b,
                            int64_t bstride, const double* __restrict__ x, int n,
                            int k, float* __restrict__ r32,
-                           unsigned long long* __restrict__ maxbits) {
+                           unsigned long long* __restrict__ maxbits, const int* skip) {
+  if (ir_skip(skip)) return;
   const int bb = blockIdx.y;
   const double* V = vals + int64_t(bb) * vals_stride;
   const double* X = x + int64_t(bb) * n * k;
@@ -483,8 +496,9 @@ __global__ void k_residual_vec(DevSym S, const double* __restrict__ vals,
                                int64_t vals_stride, const double* __restrict__ b,
                                int64_t bstride, const double* __restrict__ x, int n,
                                int k, float* __restrict__ r32,
-                               unsigned long long* __restrict__ maxbits) {
+                               unsigned long long* __restrict__ maxbits, const int* skip) {
   static_assert(RJ == 2 || RJ == 4 || RJ == 8, "2, 4 or 8 right-hand sides per thread");
+  if (ir_skip(skip)) return;
   const int bb = blockIdx.y;
   const double* V = vals + int64_t(bb) * vals_stride;
   const double* X = x + int64_t(bb) * n * k;
@@ -540,11 +554,71 @@ __global__ void k_residual_vec(DevSym S, const double* __restrict__ vals,
   }
 }
 
+// x = c (first) or x += c, folding max|c| and max|x| into the refinement
+// state (corrections only)
 __global__ void k_ir_update(const float* __restrict__ c, int64_t count,
-                            double* __restrict__ x, int first) {
+                            double* __restrict__ x, int first, IrState* ir) {
+  if (!first && ir_skip(&ir->done)) return;
+  double cmax = 0.0, xmax = 0.0;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count;
-       i += int64_t(gridDim.x) * blockDim.x)
-    x[i] = first ? double(c[i]) : x[i] + double(c[i]);
+       i += int64_t(gridDim.x) * blockDim.x) {
+    const double ci = double(c[i]);
+    const double xi = first ? ci : x[i] + ci;
+    x[i] = xi;
+    cmax = fmax(cmax, fabs(ci));
+    xmax = fmax(xmax, fabs(xi));
+  }
+  if (first) return;
+  for (int o = 16; o > 0; o >>= 1) {
+    cmax = fmax(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+  }
+  // non-negative doubles order like their bit patterns
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&ir->cmax, __double_as_longlong(cmax));
+    atomicMax(&ir->xmax, __double_as_longlong(xmax));
+  }
+}
+
+// One thread, after correction `iter` (1-based): the estimate of the error
+// of x (see IrState), the stopping decision, and DCT_ERR_IR_NOT_CONVERGED in
+// the plan's status words (supernode -1, system = iterations) when the
+// iterations stagnate or run out above the tolerance.  A NaN correction
+// counts as stagnation; a correction at the float64 rounding level of x
+// (rho <= 4 eps) ends the refinement as converged.  tol = 0 asks for a
+// fixed number of corrections: running out of them is then no error.
+__global__ void k_ir_decide(IrState* ir, int* status, unsigned long long* resid_bits,
+                            int iter, int max_iters, double tol) {
+  if (ir->done) return;
+  // the residual of this iteration becomes the plan's reported residual
+  resid_bits[0] = ir->rmax;
+  resid_bits[1] = ir->bmax;
+  ir->rmax = 0ull;
+  ir->bmax = 0ull;
+  const double c = __longlong_as_double(static_cast<long long>(ir->cmax));
+  const double x = __longlong_as_double(static_cast<long long>(ir->xmax));
+  const double rho = x > 0.0 ? c / x : (c > 0.0 ? INFINITY : 0.0);
+  const double prev = iter > 1 ? ir->rho[min(iter - 2, kIrHistory - 1)] : 1.0;
+  const double q = iter > 1 ? fmin(1.0, rho / prev) : rho;
+  const double est = rho * q;
+  ir->rho[min(iter - 1, kIrHistory - 1)] = rho;
+  ir->iters = iter;
+  ir->est = est;
+  ir->cmax = 0ull;
+  ir->xmax = 0ull;
+  const bool floor = rho <= 4.0 * 2.220446049250313e-16;
+  const bool ok = floor || (tol > 0.0 && est <= tol);
+  const bool stalled = !(rho == rho) || (iter > 1 && rho > 0.5 * prev);
+  if (ok) {
+    ir->converged = 1;
+    ir->done = 1;
+  } else if (stalled || iter >= max_iters) {
+    ir->done = 1;
+    if ((stalled || tol > 0.0) && atomicCAS(&status[0], 0, DCT_ERR_IR_NOT_CONVERGED) == 0) {
+      status[1] = -1;
+      status[2] = iter;
+    }
+  }
 }
 
 inline dim3 grid1d(int64_t total, int ny) {
@@ -572,7 +646,8 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
   SolveArgs<T> g{P->ds, nullptr, static_cast<const T*>(P->fronts), P->front_stride,
                  static_cast<const T*>(P->dinv), P->d_dinv_off, P->dinv_stride,
                  bufA, bufB, P->sym.n, k, nchunk, P->status,
-                 static_cast<const T*>(P->linv), P->d_linv_off, P->linv_stride};
+                 static_cast<const T*>(P->linv), P->d_linv_off, P->linv_stride,
+                 P->dtype == DCT_F32 && P->ir != nullptr ? &P->ir->done : nullptr};
   constexpr bool kTc = sizeof(T) == 4;
   const size_t work = sizeof(T) * size_t(P->nbatch) * P->sym.n * k;
   const double nb = P->nbatch;
@@ -703,17 +778,17 @@ cudaError_t launch_residual(dct_plan* P, const double* b, int64_t bstride,
     dim3 g = grid1d(int64_t(n) * (k / kResidualRhs), P->nbatch);
     if (kResidualRhs == 2)
       k_residual_vec<2><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
-                                                P->resid_bits);
+                                                &P->ir->rmax, &P->ir->done);
     else if (kResidualRhs == 4)
       k_residual_vec<4><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
-                                                P->resid_bits);
+                                                &P->ir->rmax, &P->ir->done);
     else
       k_residual_vec<8><<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
-                                                P->resid_bits);
+                                                &P->ir->rmax, &P->ir->done);
   } else {
     dim3 g = grid1d(int64_t(n) * k, P->nbatch);
     k_residual<<<g, kThreads, 0, st>>>(P->ds, P->vals64, nnz, b, bstride, x, n, k, r,
-                                       P->resid_bits);
+                                       &P->ir->rmax, &P->ir->done);
   }
   return cudaGetLastError();
 }
@@ -723,7 +798,13 @@ cudaError_t launch_ir_update(dct_plan* P, double* x, int k, int first,
   const int64_t count = int64_t(P->nbatch) * P->sym.n * k;
   dim3 g = grid1d(count, 1);
   k_ir_update<<<g, kThreads, 0, st>>>(static_cast<const float*>(P->bufA), count,
-                                      x, first);
+                                      x, first, P->ir);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ir_decide(dct_plan* P, int iter, cudaStream_t st) {
+  k_ir_decide<<<1, 1, 0, st>>>(P->ir, P->status, P->resid_bits, iter, P->ir_iters,
+                                P->ir_tol);
   return cudaGetLastError();
 }
 

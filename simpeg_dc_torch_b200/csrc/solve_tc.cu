@@ -94,6 +94,8 @@ template <int MODE>
 __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g) {
   pdl_wait();   // launched with launch_pdl: the predecessor's writes first
   pdl_trigger();
+  // a finished refinement: the remaining correction launches do nothing
+  if (g.skip != nullptr && *reinterpret_cast<const volatile int*>(g.skip) != 0) return;
   constexpr bool kTrans = MODE == kModeBwdGemm || MODE == kModeBwdLinv;
   constexpr bool kInv = MODE == kModeFwdLinv || MODE == kModeBwdLinv;
   constexpr int kWarps = kNT / 32;

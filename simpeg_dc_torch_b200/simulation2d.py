@@ -72,7 +72,8 @@ class TorchDC2D:
     def __init__(self, mesh, survey, nky=12, device="cuda",
                  dtype=torch.float64, active_cells=None, val_inactive=None,
                  chunk=None, singularity_removal=False, rho_primary=None,
-                 quadrature=None, refine=None, refine_fields=None):
+                 quadrature=None, refine=None, refine_fields=None,
+                 refine_tol=None):
         if quadrature is None:
             quadrature = os.environ.get("DCTORCH_QUADRATURE", "electrodes")
         if isinstance(quadrature, str) and quadrature != "electrodes":
@@ -120,7 +121,8 @@ class TorchDC2D:
                                ops.sidx, self.device, precision,
                                coords=mesh.node_grid_index()
                                if hasattr(mesh, "node_grid_index") else None,
-                               refine=refine, refine_fields=refine_fields)
+                               refine=refine, refine_fields=refine_fields,
+                               refine_tol=refine_tol)
         self.solver = self._path.solver
         if self._sr:
             # fields by the split u = rho_s u_1 + u_s (primary.py); the

@@ -23,7 +23,7 @@ class TorchDC3D:
 
     def __init__(self, mesh, survey, device="cuda", dtype=torch.float64,
                  active_cells=None, val_inactive=None, bc_type="Robin",
-                 refine=None, refine_fields=None):
+                 refine=None, refine_fields=None, refine_tol=None):
         if bc_type != "Robin":
             raise NotImplementedError("only the Robin boundary condition is built")
         self.device = torch.device(device)
@@ -47,7 +47,8 @@ class TorchDC3D:
                                ops.sidx, self.device, self.precision,
                                coords=mesh.node_grid_index()
                                if hasattr(mesh, "node_grid_index") else None,
-                               refine=refine, refine_fields=refine_fields)
+                               refine=refine, refine_fields=refine_fields,
+                               refine_tol=refine_tol)
         self.solver = self._path.solver
         self.sidx = torch.as_tensor(ops.sidx, device=self.device)
         self.iD = torch.arange(self.nD, device=self.device)

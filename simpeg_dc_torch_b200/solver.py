@@ -13,8 +13,11 @@ same pattern.
 
 Precision: a float64 solver factors and solves in float64.  A float32 solver
 factors and solves in float32 and refines every solution with residuals
-b - A x formed in float64 (`refine` iterations, default 2; 0 gives the plain
-float32 solve of the reference).
+b - A x formed in float64: at most `refine` corrections (default 2; 0 gives
+the plain float32 solve of the reference), stopping early once the
+estimated relative error is below `refine_tol` (default 1e-10).  When the
+corrections stagnate or run out above the tolerance, `check()` raises
+(status "iterative refinement did not converge").
 
 The differentiable ops `sparse_solve`, `sparse_solve_batch` and
 `sparse_solve_batch_prefactored` have the reference's contract
@@ -63,7 +66,7 @@ class _PlanSolver:
     """Shared machinery of the single and batched solvers."""
 
     def __init__(self, crow, col, n, n_rhs, nbatch, device, dtype,
-                 matrix_type, coords, refine, leaf_size):
+                 matrix_type, coords, refine, leaf_size, refine_tol=None):
         if matrix_type not in _MATRIX_TYPES:
             raise NotImplementedError(
                 f"matrix_type {matrix_type!r}: only real SPD systems are "
@@ -87,9 +90,13 @@ class _PlanSolver:
         with torch.cuda.device(self.device):
             self._plan = nat.Plan(self._sym, self.nbatch, self.n_rhs,
                                   self._code, self.device.index)
-        # refinement iterations of float32 plans (the library default is 2)
+        # refinement of float32 plans: at most `refine` corrections (the
+        # library default is 2), fewer once the estimated error is below
+        # `refine_tol` (library default 1e-10)
         self.refine = 2 if refine is None else int(refine)
         self._plan.set_refinement(self.refine)
+        self.refine_tol = 0.0 if refine_tol is None else float(refine_tol)
+        self._plan.set_refinement_tolerance(self.refine_tol)
         self.stamp = 0
 
     # ---- introspection
@@ -102,12 +109,26 @@ class _PlanSolver:
         return self._sym.info()
 
     def check(self):
-        """Synchronise and raise if a kernel reported an error (for example a
-        non-positive pivot).  Returns the last refinement residual ratio."""
+        """Synchronise and raise if a kernel reported an error since the last
+        check (a non-positive pivot, a refinement that did not converge, a
+        timed-out device wait).  Returns the last refinement residual ratio
+        max|b - A x| / max|b|."""
         code, where, res = self._plan.status(_stream_ptr(self.device))
+        if code == 5:
+            it, _, est, _ = self._plan.refinement_info(_stream_ptr(self.device))
+            raise nat.DCTError(code, "solve",
+                               f"estimated error {est:.3g} after {it} corrections "
+                               f"(tolerance {self.refine_tol:.3g}, residual "
+                               f"ratio {res:.3g})")
         if code != 0:
             raise nat.DCTError(code, "factorization", f"at supernode {where}")
         return res
+
+    def refinement_info(self):
+        """Refinement record of the last float32 solve: {"iters",
+        "converged", "est_error", "rho"} (synchronises the stream)."""
+        it, conv, est, rho = self._plan.refinement_info(_stream_ptr(self.device))
+        return {"iters": it, "converged": conv, "est_error": est, "rho": rho}
 
     # ---- numeric phases
     def _factorize(self, values):
@@ -148,9 +169,9 @@ class DCTSolver(_PlanSolver):
 
     def __init__(self, crow, col, n, n_rhs, device="cuda",
                  dtype=torch.float64, matrix_type="spd", coords=None,
-                 refine=None, leaf_size=64):
+                 refine=None, leaf_size=64, refine_tol=None):
         super().__init__(crow, col, n, n_rhs, 1, device, dtype, matrix_type,
-                         coords, refine, leaf_size)
+                         coords, refine, leaf_size, refine_tol)
 
     def factorize(self, values):
         """Numeric refactorization with new values (nnz,), same pattern."""
@@ -171,9 +192,9 @@ class DCTBatchSolver(_PlanSolver):
 
     def __init__(self, crow, col, n, n_rhs, nbatch, device="cuda",
                  dtype=torch.float64, matrix_type="spd", coords=None,
-                 refine=None, leaf_size=64):
+                 refine=None, leaf_size=64, refine_tol=None):
         super().__init__(crow, col, n, n_rhs, nbatch, device, dtype,
-                         matrix_type, coords, refine, leaf_size)
+                         matrix_type, coords, refine, leaf_size, refine_tol)
 
     def factorize(self, values):
         """values: (nbatch, nnz) -- refactorize every system."""

@@ -173,3 +173,48 @@ def test_singularity_removal_matches_reference():
         phi, grad = O.misfit_grad_2d_sr(op, m, u1, S[f"{tag}_dobs"], S[f"{tag}_w"])
         assert abs(phi - S[f"{tag}_phi"]) <= 1e-10 * abs(S[f"{tag}_phi"])
         assert O.rel(grad, S[f"{tag}_grad"]) < 1e-9
+
+
+def test_slab_solver_matches_superlu_and_reference():
+    """The block-tridiagonal slab Cholesky (the oracle's solver for the large
+    workloads) gives the reference's results on its golden problems and the
+    SuperLU solution of a float64 system to rounding."""
+    from simpeg_dc_torch_b200 import synthetic as syn
+    for name, case, three_d in (("dc2d_tiny", syn.tiny_2d, False),
+                                ("dc3d_tiny", syn.tiny_3d, True)):
+        g = golden(name)
+        mesh, _, _ = case()
+        op = _ops(g, three_d)
+        op["slab"] = O.grid_slabs(mesh.node_grid_index())
+        assert op["slab"].size == op["nN"]
+        m, dobs, w, v = g["m"], g["dobs"], g["w"], g["v"]
+        dpred = O.dpred_3d if three_d else O.dpred_2d
+        mgrad = O.misfit_grad_3d if three_d else O.misfit_grad_2d
+        jtvec = O.jtvec_3d if three_d else O.jtvec_2d
+        assert O.rel(dpred(op, m), g["dpred"]) < 1e-12
+        phi, grad = mgrad(op, m, dobs, w)
+        assert abs(phi - g["phi"]) <= 1e-12 * abs(g["phi"])
+        assert O.rel(grad, g["grad"]) < 1e-11
+        assert O.rel(jtvec(op, m, v), g["jtvec"]) < 1e-11
+    # a shared right-hand side block and a batched one on one system
+    mesh, survey, m = syn.tiny_3d()
+    from simpeg_dc_torch_b200.operators import nodal_operators
+    ops = nodal_operators(mesh, survey)
+    vals = ops.L3() @ np.exp(-m)
+    rng = np.random.default_rng(5)
+    B = rng.standard_normal((ops.nN, 3))
+    lu = O.SuperLUBatch(ops.crow, ops.col, ops.nN)
+    lu.factorize(vals)
+    sl = O.SlabCholeskyBatch(ops.crow, ops.col, ops.nN,
+                             O.grid_slabs(mesh.node_grid_index()))
+    sl.factorize(vals)
+    assert O.rel(sl.solve(B), lu.solve(B)) < 1e-12
+    assert O.rel(sl.solve(B[None]), lu.solve(B[None])) < 1e-12
+
+
+def test_slab_solver_refuses_non_adjacent_couplings():
+    crow = np.array([0, 2, 3, 5])
+    col = np.array([0, 2, 1, 0, 2])
+    import pytest
+    with pytest.raises(ValueError):
+        O.SlabCholeskyBatch(crow, col, 3, np.array([0, 1, 2]))
