@@ -283,12 +283,13 @@ def jtvec_2d(op, m, v):
     return _adjoint_2d(op, m, np.asarray(v, float))[1]
 
 
-def jvec_2d(op, m, u):
+def jvec_2d(op, m, u, fields=None):
     """J u for J = d(dpred)/dm (simulation2d.py:526-529 through
     Linearization2D.Jvec, 689-710): A_k dU_k = -A_k(dsigma) U_k with
-    dsigma = -sigma u, then J u = (Pd sum_k wq_k dU_k)[i, sidx_i]."""
+    dsigma = -sigma u, then J u = (Pd sum_k wq_k dU_k)[i, sidx_i].
+    `fields` = dpred_2d(..., return_fields=True) reuses that factorization."""
     nky = len(op["wq"])
-    d, VALS, slv, U = dpred_2d(op, m, return_fields=True)
+    d, VALS, slv, U = fields or dpred_2d(op, m, return_fields=True)
     dvals = (op["Lstack"] @ (-sigma_of(m) * np.asarray(u, float))).reshape(nky, -1)
     n = op["nN"]
     rhs = np.stack([-(sp.csr_matrix((dvals[k], op["col"], op["crow"]),

@@ -10,7 +10,10 @@ reference's solver and engine interfaces:
     TorchIP2D, TorchIP3D (linearized IP), TorchDCIP2D (joint DC + IP)
 
 Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
-discretize / SimPEG objects, which may be passed instead.
+discretize / SimPEG objects.  The engines also take a discretize
+`TensorMesh` (or any tensor mesh with its public `h` and `origin`) and
+SimPEG-shaped DC surveys (`source_list`, `location_a/b`, `locations_m/n`,
+`current`), reading only those public attributes.
 """
 __version__ = "0.1.0"
 

@@ -116,8 +116,16 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
           const double kk = base - R.ka;
           const double ni = std::min(utile, N - (base + t.t0 * utile));
           const double nj = std::min(utile, R.cend - (base + t.t1 * utile));
-          f += 2 * ni * nj * kk;
-          b += es * ((ni + nj) * kk + 2 * ni * nj);
+          if (t.t0 == t.t1) {
+            // a diagonal tile: only its lower triangle (nj <= ni columns,
+            // column c from row c down) is algorithmic work
+            const double tri = nj * ni - nj * (nj - 1) / 2;
+            f += 2 * tri * kk;
+            b += es * (ni * kk + 2 * tri);
+          } else {
+            f += 2 * ni * nj * kk;
+            b += es * ((ni + nj) * kk + 2 * ni * nj);
+          }
           if (t.t0 == 0 && t.t1 == 0 && base < ns) {
             const double w2 = std::min(dct::kPanel, ns - base);
             f += 2.0 * w2 * w2 * w2 / 3.0;

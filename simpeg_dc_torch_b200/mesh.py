@@ -2,8 +2,10 @@
 
 `TensorMesh` carries the subset of `discretize.TensorMesh` that the engines
 read: cell widths `h`, `origin`, the node/cell counts and coordinates, cell
-volumes, and node interpolation.  Any object with the same attributes (a real
-`discretize.TensorMesh` included) can be handed to the engines instead.
+volumes, and node interpolation.  The engines accept any tensor mesh that
+exposes discretize's public `h` (per-axis cell widths) and `origin` (or the
+older `x0`): `as_tensor_mesh` rebuilds it as this class, so a
+`discretize.TensorMesh` can be handed to them directly.
 
 Ordering conventions are discretize's: nodes and cells are numbered with x
 fastest, then y, then z (Fortran order).
@@ -200,3 +202,23 @@ class TensorMesh:
         P.eliminate_zeros()
         P.sum_duplicates()
         return P
+
+
+def as_tensor_mesh(mesh):
+    """This package's TensorMesh for `mesh`: the mesh itself, or a rebuild of
+    any tensor mesh that exposes discretize's public `h` (per-axis widths)
+    and `origin` (or `x0`), such as `discretize.TensorMesh`
+    (dctorch/simulation2d.py:37-40 and simulation3d.py:47-48 take those).
+    Other mesh types (a discretize `TreeMesh`, ...) raise NotImplementedError."""
+    if isinstance(mesh, TensorMesh):
+        return mesh
+    kind = str(getattr(mesh, "_meshType", "TENSOR")).upper()
+    if kind != "TENSOR" or not hasattr(mesh, "h"):
+        raise NotImplementedError(
+            f"only tensor meshes are supported (got {type(mesh).__name__})")
+    origin = getattr(mesh, "origin", None)
+    if origin is None:
+        origin = getattr(mesh, "x0", None)
+    h = [np.asarray(w, dtype=float).reshape(-1) for w in mesh.h]
+    return TensorMesh(h, origin=None if origin is None
+                      else [float(v) for v in np.asarray(origin, float)])

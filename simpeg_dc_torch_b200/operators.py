@@ -38,7 +38,8 @@ import numpy as np
 import scipy.sparse as sp
 from scipy.special import k0e, k1e
 
-from .survey import source_term
+from .mesh import as_tensor_mesh
+from .survey import receiver_projection, source_term
 
 
 @dataclass
@@ -204,9 +205,9 @@ def _boundary_faces(mesh, pos_of):
 
 
 def nodal_operators(mesh, survey) -> NodalOperators:
-    """Assemble the sigma-linear maps, sources and receivers for a tensor mesh."""
-    if getattr(mesh, "_meshType", "TENSOR").upper() != "TENSOR":
-        raise NotImplementedError("only tensor meshes are supported")
+    """Assemble the sigma-linear maps, sources and receivers for a tensor mesh
+    (this package's, or any with discretize's public `h` and `origin`)."""
+    mesh = as_tensor_mesh(mesh)
     dim = mesh.dim
     nC, nN = mesh.nC, mesh.n_nodes
     edges = _edges(mesh)
@@ -277,7 +278,7 @@ def nodal_operators(mesh, survey) -> NodalOperators:
     Pb, sidx = [], []
     for isrc, src in enumerate(survey.source_list):
         for rx in src.receiver_list:
-            P = sp.csr_matrix(rx.getP(mesh, "N"))
+            P = receiver_projection(rx, mesh)
             Pb.append(P)
             sidx += [isrc] * P.shape[0]
     Pd = sp.vstack(Pb).tocsr() if Pb else sp.csr_matrix((0, nN))

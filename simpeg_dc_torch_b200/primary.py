@@ -22,6 +22,8 @@ from __future__ import annotations
 
 import numpy as np
 
+from .survey import source_electrodes
+
 
 def unit_primary(mesh, survey, kys):
     """u_1: the unit-resistivity primary at every node, (nky, nN, nS)."""
@@ -34,9 +36,8 @@ def unit_primary(mesh, survey, kys):
     srcs = survey.source_list
     out = np.zeros((kys.size, nodes.shape[0], len(srcs)))
     for j, src in enumerate(srcs):
-        poles = [(np.asarray(src.location_a, float), 1.0)]
-        if getattr(src, "location_b", None) is not None:
-            poles.append((np.asarray(src.location_b, float), -1.0))
+        a, b = source_electrodes(src)
+        poles = [(a, 1.0)] + ([] if b is None else [(b, -1.0)])
         for loc, sign in poles:
             r = np.hypot(nodes[:, 0] - loc[0], nodes[:, 1] - loc[1])
             on_node = r < tol
@@ -54,5 +55,5 @@ def unit_primary(mesh, survey, kys):
 def source_cells(mesh, survey):
     """Cell holding each source's A electrode, (nS,)."""
     return np.array([int(np.atleast_1d(mesh.point2index(
-        np.asarray(s.location_a, float)[None, :2]))[0]) for s in survey.source_list],
+        source_electrodes(s)[0][None, :2]))[0]) for s in survey.source_list],
         dtype=np.int64)

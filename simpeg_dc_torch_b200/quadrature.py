@@ -26,16 +26,16 @@ import warnings
 
 import numpy as np
 
+from .survey import source_electrodes
+
 
 def electrode_distance_range(survey):
     """(r_min, r_max) over current/potential electrode pairs (horizontal and
     vertical coordinates only), as in dctorch/quadrature.py:38-61."""
     lo, hi = np.inf, 0.0
     for src in survey.source_list:
-        cur = [np.atleast_2d(np.asarray(src.location_a, float))]
-        lb = getattr(src, "location_b", None)
-        if lb is not None:
-            cur.append(np.atleast_2d(np.asarray(lb, float)))
+        a, b = source_electrodes(src)
+        cur = [np.atleast_2d(a)] + ([] if b is None else [np.atleast_2d(b)])
         cur = np.vstack(cur)[:, :2]
         cur = cur[np.isfinite(cur).all(axis=1)]
         for rx in src.receiver_list:

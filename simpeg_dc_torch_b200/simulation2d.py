@@ -11,11 +11,14 @@ and solved in the same launches.
 
 Precision: `dtype=torch.float64` (default) factors and solves in float64;
 `dtype=torch.float32` factors and solves in float32 with float64 iterative
-refinement (`refine` iterations, default 2).  The quadrature sum, the data
-and the misfit are float64 in both.  Data come back in the model's dtype.
+refinement (at most `refine` corrections, default 2; `refine_tol` stops
+earlier).  The quadrature sum, the data and the misfit are float64 in both.
+Data come back in the model's dtype.
 
-Not provided (out of this package's scope): singularity removal and SimPEG's
-own wavenumber fit (`quadrature="simpeg"`), both of which need SimPEG.
+Singularity removal (`singularity_removal=True`, `rho_primary`) solves for
+the field as the analytic half-space primary plus a smooth remainder (see
+`primary.py`).  Not provided: SimPEG's own wavenumber fit
+(`quadrature="simpeg"`), which needs SimPEG's optimizer run.
 """
 from __future__ import annotations
 
@@ -27,6 +30,7 @@ import torch
 
 from .primary import source_cells, unit_primary
 from ._fused import FusedDpred, FusedPath
+from .mesh import as_tensor_mesh
 from .operators import nodal_operators
 from .quadrature import (amplification, electrode_distance_range,
                          k0_quadrature, transform_error)
@@ -105,6 +109,7 @@ class TorchDC2D:
                 "max_rel_err": transform_error(kys, wq, rmin, rmax),
                 "amplification": amplification(wq), "n_used": int(kys.size)}
 
+        mesh = as_tensor_mesh(mesh)
         ops = nodal_operators(mesh, survey)
         self._ops = ops
         self.kys = np.asarray(kys, float)

@@ -14,6 +14,7 @@ import scipy.sparse as sp
 import torch
 
 from ._fused import FusedDpred, FusedPath
+from .mesh import as_tensor_mesh
 from .operators import nodal_operators
 from .simulation2d import _ActiveCells, _to_coo_tensor
 
@@ -32,6 +33,7 @@ class TorchDC3D:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.dtype = dtype
+        mesh = as_tensor_mesh(mesh)
         ops = nodal_operators(mesh, survey)
         self._ops = ops
         self.nC, self.nN, self.nS, self.nD = ops.nC, ops.nN, ops.nS, ops.nD

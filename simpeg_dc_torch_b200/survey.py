@@ -2,8 +2,10 @@
 
 Mirrors the attributes of SimPEG's `resistivity.sources`, `.receivers` and
 `.survey.Survey` that the engines read (`source_list`, `receiver_list`,
-`location_a/b`, `locations_m/n`, `current`, `nD`), so a SimPEG survey object
-can be used in place of these classes.
+`location_a/b` (or `location`), `locations_m/n` (or `locations`), `current`,
+`data_type`), so a SimPEG survey object can be used in place of these
+classes: the engines build the source terms and receiver projections from
+those attributes alone (`source_term`, `receiver_projection`).
 
 Nodal source term (SimPEG `BaseSrc.eval`, EB formulation): the current
 electrode(s) enter the right-hand side through the node interpolation matrix,
@@ -105,15 +107,46 @@ class Survey:
         return len(self.source_list)
 
 
+def source_electrodes(src):
+    """(A, B) current electrode locations of a source (SimPEG's or ours); B is
+    None for a pole (absent, None or NaN, as SimPEG writes a pole's B)."""
+    loc = getattr(src, "location_a", None)
+    a = np.asarray(src.location if loc is None else loc, float)
+    lb = getattr(src, "location_b", None)
+    if lb is None:
+        return a, None
+    lb = np.asarray(lb, float)
+    return a, (lb if np.all(np.isfinite(lb)) else None)
+
+
 def source_term(src, mesh):
-    """Nodal right-hand side of one source (SimPEG or our own class)."""
+    """Nodal right-hand side of one source (SimPEG or our own class):
+    I (P_A - P_B) through nodal interpolation, B absent for a pole
+    (SimPEG's `BaseSrc.eval` in the nodal formulation)."""
     if hasattr(src, "eval_nodal"):
         return src.eval_nodal(mesh)
-    locs = [np.asarray(src.location_a, float)]
-    lb = getattr(src, "location_b", None)
-    has_b = lb is not None and np.all(np.isfinite(np.asarray(lb, float)))
-    if has_b:
-        locs.append(np.asarray(lb, float))
+    a, b = source_electrodes(src)
+    locs = [a] if b is None else [a, b]
     P = mesh.get_interpolation_matrix(np.vstack(locs), "N").toarray()
     cur = float(getattr(src, "current", 1.0))
-    return cur * (P[0] - P[1]) if has_b else cur * P[0]
+    return cur * (P[0] - P[1]) if b is not None else cur * P[0]
+
+
+def receiver_projection(rx, mesh):
+    """P (nD_rx, nN) of one receiver: P_M - P_N for a dipole, P_M for a pole,
+    from the public locations of a SimPEG receiver or one of ours (what
+    SimPEG's `rx.getP(mesh, "N")` returns, dctorch/simulation2d.py:236-244)."""
+    import scipy.sparse as sp
+    lm = getattr(rx, "locations_m", None)
+    locs = getattr(rx, "locations", None)
+    if lm is None:
+        lm = locs[0] if isinstance(locs, (list, tuple)) else locs
+    ln = getattr(rx, "locations_n", None)
+    if ln is None and isinstance(locs, (list, tuple)) and len(locs) == 2:
+        ln = locs[1]
+    P = mesh.get_interpolation_matrix(np.atleast_2d(np.asarray(lm, float)), "N")
+    if ln is not None:
+        ln = np.atleast_2d(np.asarray(ln, float))
+        if np.all(np.isfinite(ln)):
+            P = P - mesh.get_interpolation_matrix(ln, "N")
+    return sp.csr_matrix(P)

@@ -92,3 +92,100 @@ def test_half_space_2p5d_matches_analytic():
                                     + 1 / r(b, N)) / (2 * np.pi))
     err = np.abs(d / np.array(truth) - 1)
     assert np.median(err) < 0.03 and err.max() < 0.1
+
+
+class _DiscretizeLikeMesh:
+    """Only the public attributes a discretize.TensorMesh has: h, origin, dim,
+    _meshType (no private helpers of this package's TensorMesh)."""
+    _meshType = "TENSOR"
+
+    def __init__(self, h, origin):
+        self.h = tuple(np.asarray(w, float) for w in h)
+        self.origin = np.asarray(origin, float)
+        self.dim = len(self.h)
+
+
+class _SimpegLikeDipoleRx:
+    def __init__(self, m, n):
+        self.locations_m, self.locations_n = np.asarray(m), np.asarray(n)
+        self.data_type = "volt"
+
+    @property
+    def nD(self):
+        return self.locations_m.shape[0]
+
+
+class _SimpegLikePoleRx:
+    def __init__(self, m):
+        self.locations = np.asarray(m)
+        self.data_type = "volt"
+
+    @property
+    def nD(self):
+        return self.locations.shape[0]
+
+
+class _SimpegLikeSrc:
+    def __init__(self, rxs, a, b=None, current=1.0):
+        self.receiver_list = rxs
+        self.location_a = np.asarray(a, float)
+        # SimPEG writes a pole source's B electrode as NaN
+        self.location_b = (np.full_like(self.location_a, np.nan) if b is None
+                           else np.asarray(b, float))
+        self.current = current
+
+
+class _SimpegLikeSurvey:
+    def __init__(self, srcs):
+        self.source_list = srcs
+
+    @property
+    def nD(self):
+        return sum(rx.nD for s in self.source_list for rx in s.receiver_list)
+
+
+def _mirror(survey):
+    """A SimPEG-shaped copy of one of this package's surveys."""
+    out = []
+    for src in survey.source_list:
+        rxs = []
+        for rx in src.receiver_list:
+            if rx.locations_n is None:
+                rxs.append(_SimpegLikePoleRx(rx.locations_m))
+            else:
+                rxs.append(_SimpegLikeDipoleRx(rx.locations_m, rx.locations_n))
+        out.append(_SimpegLikeSrc(rxs, src.location_a, src.location_b, src.current))
+    return _SimpegLikeSurvey(out)
+
+
+def test_engines_accept_discretize_and_simpeg_shaped_objects():
+    """The operators built from a mesh that has only discretize's public
+    attributes and a survey that has only SimPEG's equal the ones built from
+    this package's own classes (the reference engines take discretize /
+    SimPEG objects, dctorch/simulation2d.py:37-40, simulation3d.py:47-48)."""
+    from simpeg_dc_torch_b200 import synthetic as syn
+    from simpeg_dc_torch_b200.mesh import as_tensor_mesh
+    from simpeg_dc_torch_b200.quadrature import electrode_distance_range
+    for case in (syn.tiny_2d, syn.tiny_3d):
+        mesh, survey, _ = case()
+        dmesh = _DiscretizeLikeMesh(mesh.h, mesh.origin)
+        ssurv = _mirror(survey)
+        a = nodal_operators(mesh, survey)
+        b = nodal_operators(dmesh, ssurv)
+        assert np.array_equal(a.crow, b.crow) and np.array_equal(a.col, b.col)
+        for M, N in ((a.L_edge, b.L_edge), (a.L_node, b.L_node), (a.q, b.q),
+                     (a.Pd, b.Pd)):
+            assert abs(M - N).max() == 0.0
+        assert np.array_equal(a.sidx, b.sidx)
+        L = a.L3() if mesh.dim == 3 else a.L_ky(0.1)
+        Lb = b.L3() if mesh.dim == 3 else b.L_ky(0.1)
+        assert abs(L - Lb).max() == 0.0
+        assert electrode_distance_range(survey) == electrode_distance_range(ssurv)
+        assert np.array_equal(as_tensor_mesh(dmesh).node_grid_index(),
+                              mesh.node_grid_index())
+
+    class _Tree:
+        _meshType = "TREE"
+        h = ()
+    with pytest.raises(NotImplementedError):
+        as_tensor_mesh(_Tree())
