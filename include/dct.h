@@ -102,11 +102,13 @@ void dct_plan_destroy(dct_plan* plan);
  * solve; each correction i adds c_i = A_32^{-1} (b - A x) with the residual
  * formed in float64.  rho_i = max|c_i| / max|x_i| estimates the relative
  * error of the previous iterate, so rho_i * min(1, rho_i / rho_{i-1})
- * (rho_1^2 for the first) estimates that of x_i.  Refinement stops once that
- * estimate is <= tol (default 1e-10); when the corrections stagnate
- * (rho_i > rho_{i-1} / 2, or NaN) or the iterations run out above tol, the
- * plan's status words record DCT_ERR_IR_NOT_CONVERGED (read by
- * dct_check_status, `where` = -1).  The decision is taken on the device: the
+ * (rho_1^2 for the first) estimates that of x_i.  With tol > 0 refinement
+ * stops once that estimate is <= tol, and when the corrections stagnate
+ * (rho_i > rho_{i-1} / 2) or the iterations run out above tol, the plan's
+ * status words record DCT_ERR_IR_NOT_CONVERGED (read by dct_check_status,
+ * `where` = -1).  tol = 0 (the default) runs the fixed number of
+ * corrections, ending early only at a stall or at float64 rounding.  A NaN
+ * correction is always recorded as DCT_ERR_IR_NOT_CONVERGED.  The decision is taken on the device: the
  * launches of corrections that are not needed return at entry and the host
  * never waits.  Replaces the fixed precision of CuDSSSolver's float32 solves
  * (dctorch/solver.py:122-135), which has no refinement. */

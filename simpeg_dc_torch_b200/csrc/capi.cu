@@ -58,10 +58,14 @@ int alloc(dct_plan* P, size_t bytes, void** out, const char* what) {
 
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// Tiles of a trailing update start at `base` (float64) or at base & ~7
+// (float32: the 8-row grid of the split panel images, update_tc.cu).
+int update_origin(int base, bool align8) { return align8 ? (base & ~7) : base; }
+
 // ---- schedules ------------------------------------------------------------
 // Algorithmic work of each launch (see dct::Schedule).  es = element size.
 void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
-                    int utile, int bpan) {
+                    int utile, int bpan, bool align8) {
   sc->flops.assign(sc->launches.size(), 0.0);
   sc->bytes.assign(sc->launches.size(), 0.0);
   sc->bytes_rhs.assign(sc->launches.size(), 0.0);
@@ -114,8 +118,12 @@ void account_factor(const dct::Symbolic& S, dct::Schedule* sc, double es,
           const int base = c0 + w;
           const dct::UpdateRange R = dct::update_range(t.p, ns, N, bpan);
           const double kk = base - R.ka;
-          const double ni = std::min(utile, N - (base + t.t0 * utile));
-          const double nj = std::min(utile, R.cend - (base + t.t1 * utile));
+          // the tile's rows and columns from `base` on that it updates
+          const int R0 = update_origin(base, align8);
+          const int ri = std::max(base, R0 + t.t0 * utile);
+          const int rj = std::max(base, R0 + t.t1 * utile);
+          const double ni = std::min(R0 + (t.t0 + 1) * utile, N) - ri;
+          const double nj = std::min(R0 + (t.t1 + 1) * utile, R.cend) - rj;
           if (t.t0 == t.t1) {
             // a diagonal tile: only its lower triangle (nj <= ni columns,
             // column c from row c down) is algorithmic work
@@ -226,7 +234,7 @@ int update_tile(int dtype) { return dtype == DCT_F64 ? dct::kUpdateTile : 128; }
 int update_block(int dtype) { return dtype == DCT_F64 ? 1 : dct::kUpdateBlockPanels; }
 
 void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int bpan,
-                           dct::Schedule* out) {
+                           bool align8, dct::Schedule* out) {
   auto& T = out->tasks;
   auto& L = out->launches;
   for (int lv = 0; lv < S.nlevels; ++lv) {
@@ -291,8 +299,10 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int
         if (c0 >= ns) continue;
         int w = std::min(dct::kPanel, ns - c0);
         const dct::UpdateRange R = dct::update_range(p, ns, N, bpan);
-        int nti = ceil_div(N - c0 - w, utile);
-        int ntj = ceil_div(R.cend - c0 - w, utile);
+        const int R0 = update_origin(c0 + w, align8);
+        // no tile when nothing lies beyond the panel (R0 may sit above it)
+        int nti = N > c0 + w ? ceil_div(N - R0, utile) : 0;
+        int ntj = R.cend > c0 + w ? ceil_div(R.cend - R0, utile) : 0;
         for (int i = 0; i < nti; ++i)
           for (int j = 0; j <= i && j < ntj; ++j) T.push_back({s, p, i, j});
       }
@@ -655,7 +665,8 @@ int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t whic
     return fail(DCT_ERR_ARG, "bad arguments");
   dct::Schedule f, fw, bw, iv;
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(h->sym, small_max, update_tile(dtype), update_block(dtype), &f);
+  build_factor_schedule(h->sym, small_max, update_tile(dtype), update_block(dtype),
+                        dtype == DCT_F32, &f);
   build_solve_schedules(h->sym, dtype, &fw, &bw);
   std::vector<int64_t> off;
   int64_t tot = 0;
@@ -737,7 +748,8 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
       (rc = upload(P, S.in_crow, &D.crow)) || (rc = upload(P, S.in_col, &D.col)))
     return bail(rc);
   const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(S, small_max, update_tile(dtype), update_block(dtype), &P->fact);
+  build_factor_schedule(S, small_max, update_tile(dtype), update_block(dtype),
+                        dtype == DCT_F32, &P->fact);
   P->update_bpan = update_block(dtype);
   build_solve_schedules(S, dtype, &P->fwd, &P->bwd);
   std::vector<int64_t> dinv_off;
@@ -754,8 +766,34 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
     if ((rc = upload(P, linv_off, &d))) return bail(rc);
     P->d_linv_off = d;
   }
+  if (dtype == DCT_F32) {
+    // split images of every panel of the large fronts (update_tc.cu)
+    std::vector<int32_t> pan_first(S.nsuper + 1, 0);
+    std::vector<int64_t> img_off;
+    int64_t acc = 0;
+    for (int s = 0; s < S.nsuper; ++s) {
+      pan_first[s] = int32_t(img_off.size());
+      const int ns = S.ns(s), N = S.front_n[s];
+      for (int q = 0; q * dct::kPanel < ns; ++q) {
+        img_off.push_back(acc);
+        if (N > small_max) acc += int64_t(4) * dct::img_groups(q, ns, N) * 256;
+      }
+    }
+    pan_first[S.nsuper] = int32_t(img_off.size());
+    img_off.push_back(acc);
+    const int64_t* d_off = nullptr;
+    const int32_t* d_pf = nullptr;
+    if ((rc = upload(P, img_off, &d_off)) || (rc = upload(P, pan_first, &d_pf))) return bail(rc);
+    void* img = nullptr;
+    if ((rc = alloc(P, sizeof(float) * size_t(acc) * nbatch, &img, "panel images")))
+      return bail(rc);
+    // padding rows and the columns beyond a narrow panel are never written
+    if (cudaMemset(img, 0, sizeof(float) * size_t(acc) * nbatch) != cudaSuccess)
+      return bail(fail(DCT_ERR_CUDA, "cudaMemset (panel images)"));
+    P->img = dct::ImgArgs{static_cast<float*>(img), d_off, d_pf, acc};
+  }
   account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype),
-                 update_block(dtype));
+                 update_block(dtype), dtype == DCT_F32);
   account_solve(S, &P->fwd, double(esize(dtype)));
   account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||

@@ -117,6 +117,37 @@ __host__ __device__ inline UpdateRange update_range(int p, int ns, int N, int bp
   return r;
 }
 
+// Split images of the factor panels of large float32 fronts, the operands of
+// the tensor-core trailing update (update_tc.cu).  Panel q of a supernode
+// (columns c0 = 64 q .. c0 + w) has an image of the rows from
+// R0 = c0 + (w & ~7) (8-aligned, at most 7 rows above the first row below
+// the panel) down to the front's last row, in groups of 8 rows, plus 16
+// groups of zero padding so that any 128-row window that starts below the
+// front's last row lies inside it.  Each element is stored twice, hi =
+// tf32(x) and lo = x - hi, in the tensor cores' K-major layout without
+// swizzle: [hl][K stage of 32 columns][8-row group][K core of 4][row of 8]
+// [column of 4] floats, so 128 rows x 32 columns of one of hi/lo are 16 KB
+// contiguous (core matrices 128 B apart along K, 8-row groups 1 KB apart).
+__host__ __device__ inline int img_origin(int q, int ns) {
+  const int c0 = q * kPanel;
+  const int w = ns - c0 < kPanel ? ns - c0 : kPanel;
+  return c0 + (w & ~7);
+}
+__host__ __device__ inline int img_groups(int q, int ns, int N) {
+  return (N - img_origin(q, ns) + 7) / 8 + 16;
+}
+// float offset of (hl, K stage, group g, column k of the stage, row r8 of the
+// group) in a panel image of G groups
+__host__ __device__ inline int64_t img_index(int G, int hl, int stage, int g, int k, int r8) {
+  return (int64_t(hl * 2 + stage) * G + g) * 256 + (k >> 2) * 32 + r8 * 4 + (k & 3);
+}
+struct ImgArgs {
+  float* img;                // nbatch * stride floats
+  const int64_t* off;        // per panel (pan_first[s] + q): first float
+  const int32_t* pan_first;  // per supernode: index of its first panel
+  int64_t stride;            // floats per system
+};
+
 // Programmatic dependent launch for the long chains of dependent launches
 // (panel TRSM <-> trailing update, the substitution products): a kernel
 // launched with launch_pdl may be scheduled while its predecessor in the
@@ -212,6 +243,7 @@ struct dct_plan {
   unsigned long long* resid_bits = nullptr;  // device: max|r|, max|b|
   int factored = 0;
   int64_t stamp = 0;
+  dct::ImgArgs img{};              // f32 plans: split panel images (large fronts)
   int ir_iters = 2;                // most refinement iterations of f32 plans
   double ir_tol = 0.0;             // stop once the estimated error is below (0: fixed count)
   dct::IrState* ir = nullptr;      // device: refinement state of the last solve
@@ -248,6 +280,9 @@ struct SolveArgs {
 // one launch of a tensor-core substitution kind (kFwdLinvTc .. kBwdLinvTc)
 cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g, int64_t count,
                             int nbatch, cudaStream_t st);
+// one launch of the float32 trailing update (update_tc.cu)
+cudaError_t launch_update_tc(dct_plan* P, const PanelTask* tasks, int64_t count,
+                             cudaStream_t st);
 // records the message returned by dct_last_error() for this thread
 void set_last_error(const char* msg);
 cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,

@@ -584,9 +584,10 @@ __global__ void k_ir_update(const float* __restrict__ c, int64_t count,
 // of x (see IrState), the stopping decision, and DCT_ERR_IR_NOT_CONVERGED in
 // the plan's status words (supernode -1, system = iterations) when the
 // iterations stagnate or run out above the tolerance.  A NaN correction
-// counts as stagnation; a correction at the float64 rounding level of x
-// (rho <= 4 eps) ends the refinement as converged.  tol = 0 asks for a
-// fixed number of corrections: running out of them is then no error.
+// always counts as a failure; a correction at the float64 rounding level of
+// x (rho <= 4 eps) ends the refinement as converged.  tol = 0 asks for a
+// fixed number of corrections: a stall or running out of them then just
+// ends the refinement.
 __global__ void k_ir_decide(IrState* ir, int* status, unsigned long long* resid_bits,
                             int iter, int max_iters, double tol) {
   if (ir->done) return;
@@ -606,15 +607,18 @@ __global__ void k_ir_decide(IrState* ir, int* status, unsigned long long* resid_
   ir->est = est;
   ir->cmax = 0ull;
   ir->xmax = 0ull;
+  const bool nan = !(rho == rho);
   const bool floor = rho <= 4.0 * 2.220446049250313e-16;
-  const bool ok = floor || (tol > 0.0 && est <= tol);
-  const bool stalled = !(rho == rho) || (iter > 1 && rho > 0.5 * prev);
+  const bool ok = !nan && (floor || (tol > 0.0 && est <= tol));
+  const bool stalled = nan || (iter > 1 && rho > 0.5 * prev);
   if (ok) {
     ir->converged = 1;
     ir->done = 1;
   } else if (stalled || iter >= max_iters) {
+    // a stall at the accuracy float64 residuals allow is no error under a
+    // fixed count (tol = 0); a NaN always is
     ir->done = 1;
-    if ((stalled || tol > 0.0) && atomicCAS(&status[0], 0, DCT_ERR_IR_NOT_CONVERGED) == 0) {
+    if ((nan || tol > 0.0) && atomicCAS(&status[0], 0, DCT_ERR_IR_NOT_CONVERGED) == 0) {
       status[1] = -1;
       status[2] = iter;
     }

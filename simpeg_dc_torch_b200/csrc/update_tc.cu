@@ -1,0 +1,265 @@
+// Float32 trailing update of the large fronts on the tensor cores,
+// F_ij -= L_i L_j^T over 128 x 128 tiles, with the operands streamed from
+// the split panel images (see img_origin in dct_internal.h) that the panel
+// TRSM writes once per panel.
+//
+// One CTA per output tile, warp-specialised:
+//   warp 0    one thread issues the bulk copies (cp.async.bulk ... complete_tx)
+//             of each K stage -- 32 columns of the hi and lo images of the
+//             tile's row block i and column block j, 16 KB each, contiguous in
+//             the images -- into a three-stage ring, each stage guarded by a
+//             "full" mbarrier (transaction bytes) and an "empty" one;
+//   warp 1    allocates TMEM and one thread issues tcgen05.mma kind::tf32 for
+//             each stage (3xTF32: hi*hi + hi*lo + lo*hi; Markidis et al. 2018,
+//             Ootomo & Yokota 2022), then commits to the stage's "empty"
+//             barrier so the ring slot can be refilled;
+//   warps 2-5 wait for the last commit, read the accumulators from TMEM (one
+//             row per thread) and subtract them from the tile in place.
+// No thread converts or stages operands: the split happens once per panel,
+// not once per tile and K stage.
+//
+// K is the column range [ka, base) of update_range: one panel for the
+// narrow updates inside a block of panels, up to four for the update of the
+// columns beyond the block.  Each panel accumulates in its own TMEM
+// accumulator (128 columns; all 512) and the panels' products are
+// subtracted one at a time, each rounded to float32, as in a
+// panel-by-panel update.  Tiles start at R0 = base & ~7 (the 8-row grid of
+// the images); rows and columns above `base` belong to the panel itself and
+// are left untouched, as are columns at or beyond the update's end and, in
+// diagonal tiles, the upper triangle.  The CTA of tile (0, 0) then factors
+// the next panel's diagonal block.  Every wait is bounded (kTcWaitLimit
+// polls): on timeout DCT_ERR_DEVICE_TIMEOUT is recorded and the CTA returns.
+#include <cuda_runtime.h>
+
+#include "dct_internal.h"
+#include "factor_diag.cuh"
+#include "tc_common.cuh"
+
+namespace dct {
+namespace {
+
+constexpr int kUThreads = 192;
+constexpr int kUStages = 3;
+constexpr int kUChunk = 16384;              // 128 rows x 32 columns, hi or lo
+constexpr int kUStageBytes = 4 * kUChunk;   // A hi, A lo, B hi, B lo
+constexpr uint32_t kULbo = 128, kUSbo = 1024;
+constexpr int kUAcc = 4;                    // accumulators: one per panel
+constexpr size_t kUSmem = size_t(kUStages) * kUStageBytes + 128;
+static_assert(kUAcc * 128 <= 512, "TMEM columns of one SM");
+static_assert(size_t(kUStages) * kUStageBytes >= sizeof(float) * kDiagSmemElems,
+              "the ring also holds factor_diag's workspace");
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// bulk global -> shared copy whose completion is counted on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// one thread: bounded wait for phase `parity`
+__device__ __forceinline__ bool mbar_wait1(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kTcWaitLimit; ++it)
+    if (mbar_try_wait_sleep(smem_u32(bar), parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void flag_timeout(int* status, int s, int b) {
+  if (atomicCAS(&status[0], 0, DCT_ERR_DEVICE_TIMEOUT) == 0) {
+    status[1] = s;
+    status[2] = b;
+  }
+}
+
+__global__ void __launch_bounds__(kUThreads, 1)
+k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
+            int64_t front_stride, float* dinv, const int64_t* dinv_off, int64_t dinv_stride,
+            int bpan, int* status, ImgArgs im) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
+  // the bulk copies and the MMA descriptors need 16-byte alignment
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kUStages * kUStageBytes);
+  uint64_t* empty = full + kUStages;
+  uint64_t* done = empty + kUStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  const PanelTask tk = tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s;
+  const int N = S.front_n[s];
+  const int ns = S.sn_first[s + 1] - S.sn_first[s];
+  const int c0 = tk.p * kPanel;
+  const int w = min(kPanel, ns - c0);
+  const int base = c0 + w;
+  float* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  float* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tk.t0 < 0) {
+    factor_diag<float, kUThreads>(F, N, c0, w, reinterpret_cast<float*>(smem_raw),
+                                  Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
+    return;
+  }
+  const UpdateRange R = update_range(tk.p, ns, N, bpan);
+  const int R0 = base & ~7;
+  const int ri = R0 + tk.t0 * kTcM, rj = R0 + tk.t1 * kTcN;
+  const bool diag = tk.t0 == tk.t1;
+  const int jn = min(kTcN, R.cend - rj);    // tile columns that can be written
+  const int np = (jn + 15) & ~15;           // MMA N: a multiple of 16
+  const int nst = (base - R.ka + 31) / 32;
+  const int nacc = (base - R.ka + kPanel - 1) / kPanel;
+
+  if (warp == 1) tmem_alloc(tmem_slot, kUAcc * 128);
+  if (tid == 0) {
+    for (int i = 0; i < kUStages; ++i) {
+      mbar_init(&full[i]);
+      mbar_init(&empty[i]);
+    }
+    mbar_init(done);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const float* img = im.img + int64_t(b) * im.stride;
+  const int pan0 = im.pan_first[s];
+  // the 16 KB chunk of rows row0 .. row0 + 127, K stage st, hi (0) / lo (1)
+  auto chunk = [&](int row0, int st, int hl) -> const float* {
+    const int kcol = R.ka + 32 * st;
+    const int q = kcol / kPanel;
+    const int G = img_groups(q, ns, N);
+    const int g0 = (row0 - img_origin(q, ns)) >> 3;
+    return img + im.off[pan0 + q] + img_index(G, hl, (kcol % kPanel) / 32, g0, 0, 0);
+  };
+
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {
+      const uint32_t bytes = diag ? 2 * kUChunk : 4 * kUChunk;
+      int st = 0;
+      for (; st < nst; ++st) {
+        const int slot = st % kUStages;
+        if (st >= kUStages && !mbar_wait1(&empty[slot], uint32_t(st / kUStages - 1) & 1u)) {
+          ok = false;
+          break;
+        }
+        unsigned char* dst = smem_raw + slot * kUStageBytes;
+        mbar_expect_tx(&full[slot], bytes);
+        bulk_g2s(dst, chunk(ri, st, 0), kUChunk, &full[slot]);
+        bulk_g2s(dst + kUChunk, chunk(ri, st, 1), kUChunk, &full[slot]);
+        if (!diag) {
+          bulk_g2s(dst + 2 * kUChunk, chunk(rj, st, 0), kUChunk, &full[slot]);
+          bulk_g2s(dst + 3 * kUChunk, chunk(rj, st, 1), kUChunk, &full[slot]);
+        }
+      }
+      // no copy may still be writing this CTA's shared memory at exit: the
+      // last stages' copies have landed once their barriers complete
+      for (int t = max(0, st - kUStages); t < st; ++t)
+        if (!mbar_wait1(&full[t % kUStages], uint32_t(t / kUStages) & 1u)) ok = false;
+      if (!ok) flag_timeout(status, s, b);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = umma_idesc_tf32(kTcM, np);
+      for (int st = 0; st < nst; ++st) {
+        const int slot = st % kUStages;
+        if (!mbar_wait1(&full[slot], uint32_t(st / kUStages) & 1u)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t ah = smem_u32(smem_raw + slot * kUStageBytes);
+        const uint32_t al = ah + kUChunk;
+        const uint32_t bh = diag ? ah : ah + 2 * kUChunk;
+        const uint32_t bl = diag ? al : ah + 3 * kUChunk;
+        const int kcol = R.ka + 32 * st;
+        const uint32_t acc = tmem + uint32_t(((kcol - R.ka) / kPanel) * 128);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const uint32_t ko = uint32_t(kk) * 2 * kULbo;
+          const uint64_t dah = umma_desc(ah + ko, kULbo, kUSbo);
+          const uint64_t dal = umma_desc(al + ko, kULbo, kUSbo);
+          const uint64_t dbh = umma_desc(bh + ko, kULbo, kUSbo);
+          const uint64_t dbl = umma_desc(bl + ko, kULbo, kUSbo);
+          const bool fresh = (kcol % kPanel) == 0 && kk == 0;
+          umma_tf32(acc, dah, dbh, idesc, fresh ? 0u : 1u);
+          umma_tf32(acc, dah, dbl, idesc, 1u);
+          umma_tf32(acc, dal, dbh, idesc, 1u);
+        }
+        umma_commit(&empty[slot]);
+      }
+      if (!ok) flag_timeout(status, s, b);
+      // tracks every MMA issued before it, also after a timeout
+      umma_commit(done);
+    }
+  } else {
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile rows
+    bool got = false;
+    if (lane == 0) got = mbar_wait1(done, 0);
+    got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!got) {
+      ok = false;
+      if (lane == 0) flag_timeout(status, s, b);
+    } else {
+      const int quarter = warp & 3;
+      const int row = ri + quarter * 32 + lane;
+      const bool row_ok = row >= base && row < N;
+      float* dst = F + min(row, N - 1);
+      for (int cb = 0; cb < np; cb += 32) {
+        float cur[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const int col = rj + cb + c;
+          const bool in = row_ok && cb + c < jn && col >= base && (!diag || col <= row);
+          cur[c] = in ? dst[int64_t(col) * N] : 0.0f;
+        }
+        for (int a = 0; a < nacc; ++a) {
+          uint32_t v[32];
+          tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(a * 128 + cb), v);
+#pragma unroll
+          for (int c = 0; c < 32; ++c) cur[c] -= __uint_as_float(v[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const int col = rj + cb + c;
+          if (row_ok && cb + c < jn && col >= base && (!diag || col <= row))
+            dst[int64_t(col) * N] = cur[c];
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+  if (warp == 1) tmem_dealloc(tmem, kUAcc * 128);
+  if (all_ok && tk.t0 == 0 && tk.t1 == 0 && base < ns) {
+    __syncthreads();   // this CTA's updates of the block are complete
+    factor_diag<float, kUThreads>(F, N, base, min(kPanel, ns - base),
+                                  reinterpret_cast<float*>(smem_raw),
+                                  Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_update_tc(dct_plan* P, const PanelTask* tasks, int64_t count,
+                             cudaStream_t st) {
+  cudaError_t e = cudaFuncSetAttribute(k_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kUSmem));
+  if (e != cudaSuccess) return e;
+  dim3 grid(static_cast<unsigned>(count), static_cast<unsigned>(P->nbatch));
+  return launch_pdl(k_update_tc, grid, dim3(kUThreads), kUSmem, st, P->ds, tasks,
+                    static_cast<float*>(P->fronts), P->front_stride,
+                    static_cast<float*>(P->dinv), P->d_dinv_off, P->dinv_stride,
+                    P->update_bpan, P->status, P->img);
+}
+
+}  // namespace dct

@@ -14,10 +14,11 @@ same pattern.
 Precision: a float64 solver factors and solves in float64.  A float32 solver
 factors and solves in float32 and refines every solution with residuals
 b - A x formed in float64: at most `refine` corrections (default 2; 0 gives
-the plain float32 solve of the reference), stopping early once the
-estimated relative error is below `refine_tol` (default 1e-10).  When the
-corrections stagnate or run out above the tolerance, `check()` raises
-(status "iterative refinement did not converge").
+the plain float32 solve of the reference).  With `refine_tol` > 0 the
+refinement stops once the estimated relative error of the solution is below
+it, and when the corrections stagnate or run out above it `check()` raises
+(status "iterative refinement did not converge"); `refine_tol` = 0 (the
+default) runs the fixed number of corrections.
 
 The differentiable ops `sparse_solve`, `sparse_solve_batch` and
 `sparse_solve_batch_prefactored` have the reference's contract
@@ -92,7 +93,7 @@ class _PlanSolver:
                                   self._code, self.device.index)
         # refinement of float32 plans: at most `refine` corrections (the
         # library default is 2), fewer once the estimated error is below
-        # `refine_tol` (library default 1e-10)
+        # `refine_tol` (0, the library default: a fixed count)
         self.refine = 2 if refine is None else int(refine)
         self._plan.set_refinement(self.refine)
         self.refine_tol = 0.0 if refine_tol is None else float(refine_tol)

@@ -59,6 +59,61 @@ def _factor_diag(S, F, s, c0, w, dinv):
     dinv[(s, c0 // PANEL)] = np.linalg.inv(L)
 
 
+SMALL_F32 = 224      # largest front of the single-CTA float32 kernel
+
+
+def img_origin(q, ns):
+    """First row of panel q's split image (libdct's dct::img_origin)."""
+    c0 = q * PANEL
+    return c0 + (min(PANEL, ns - c0) & ~7)
+
+
+def img_groups(q, ns, N):
+    return (N - img_origin(q, ns) + 7) // 8 + 16
+
+
+def img_index(G, hl, stage, g, k, r8):
+    return ((hl * 2 + stage) * G + g) * 256 + (k >> 2) * 32 + r8 * 4 + (k & 3)
+
+
+def image_offsets(S):
+    """{(s, q): first float of panel q's image} of the large fronts and the
+    total size (the plan's layout, capi.cu)."""
+    off, acc = {}, 0
+    for s in range(S.nsuper):
+        ns, N = S.ns(s), int(S.front_n[s])
+        for q in range(-(-ns // PANEL)):
+            off[(s, q)] = acc
+            if N > SMALL_F32:
+                acc += 4 * img_groups(q, ns, N) * 256
+    return off, acc
+
+
+# element (m, k) of a 128-row x 32-column image chunk
+_CHUNK_M, _CHUNK_K = np.meshgrid(np.arange(128), np.arange(32), indexing="ij")
+_CHUNK_IDX = ((_CHUNK_M // 8) * 256 + (_CHUNK_K // 4) * 32 + (_CHUNK_M % 8) * 4
+              + _CHUNK_K % 4)
+
+
+def _image_operand(dinv, s, ns, N, row0, ka, nst):
+    """The (128, 32 nst) operand the tensor-core update streams from the
+    panel images for tile rows row0 .. row0 + 127 and K stages of 32 columns
+    from ka, with every chunk bounds-checked against its panel's image."""
+    img = dinv[("img", 0)]
+    parts = []
+    for st in range(nst):
+        kcol = ka + 32 * st
+        q, h = kcol // PANEL, (kcol % PANEL) // 32
+        G, R0q = img_groups(q, ns, N), img_origin(q, ns)
+        assert row0 >= R0q and (row0 - R0q) % 8 == 0
+        off = dinv[("imgoff", s, q)]
+        lo = off + img_index(G, 0, h, 0, 0, 0)
+        start = off + img_index(G, 0, h, (row0 - R0q) // 8, 0, 0)
+        assert lo <= start and start + 4096 <= lo + G * 256, "chunk outside its image"
+        parts.append(img[start + _CHUNK_IDX])
+    return np.hstack(parts)
+
+
 def update_range(p, ns, N, bpan):
     """K columns [ka, base) and last column cend of the trailing update after
     panel p when panels are grouped in blocks of bpan (libdct's
@@ -122,6 +177,17 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE, bpan=1):
         nr = min(PANEL, N - r0)
         assert nr > 0
         F[r0:r0 + nr, c0:c0 + w] = F[r0:r0 + nr, c0:c0 + w] @ Di.T
+        if utile == TCTILE:
+            # float32 plans: the split image of these rows (hi part; the
+            # replay is exact, so lo stays zero)
+            img, off = dinv[("img", 0)], dinv[("imgoff", s, p)]
+            G, R0q = img_groups(p, ns, N), img_origin(p, ns)
+            rr, cc = np.meshgrid(np.arange(nr), np.arange(w), indexing="ij")
+            gr = r0 + rr - R0q
+            assert gr.min() >= 0 and gr.max() < 8 * (G - 16)
+            idx = off + img_index(G, 0, cc >> 5, gr >> 3, cc & 31, gr & 7)
+            assert idx.max() < off + 2 * G * 256
+            img[idx] = F[r0:r0 + nr, c0:c0 + w]
     elif kind == LUPDATE:
         c0 = p * PANEL
         w = min(PANEL, ns - c0)
@@ -130,11 +196,35 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE, bpan=1):
             _factor_diag(S, F, s, c0, w, dinv)
             return
         ka, cend = update_range(p, ns, N, bpan)
-        ri, rj = base + t0 * utile, base + t1 * utile
+        # float32 plans (128-row tensor-core tiles) start the tiles at
+        # base & ~7, the 8-row grid of the split panel images, and update
+        # only the rows and columns from base on (update_tc.cu)
+        R0 = base & ~7 if utile == TCTILE else base
+        ri, rj = R0 + t0 * utile, R0 + t1 * utile
         assert ri < N and rj < cend and t0 >= t1
-        ni, nj = min(utile, N - ri), min(utile, cend - rj)
-        F[ri:ri + ni, rj:rj + nj] -= (F[ri:ri + ni, ka:base]
-                                      @ F[rj:rj + nj, ka:base].T)
+        ri, rj = max(ri, base), max(rj, base)
+        ni = min(R0 + (t0 + 1) * utile, N) - ri
+        nj = min(R0 + (t1 + 1) * utile, cend) - rj
+        assert ni > 0 and nj > 0
+        upd = F[ri:ri + ni, ka:base] @ F[rj:rj + nj, ka:base].T
+        if utile == TCTILE:
+            # the tensor-core kernel's operands come from the panel images:
+            # they must hold exactly these rows of L
+            nst = (base - ka + 31) // 32
+            Ai = _image_operand(dinv, s, ns, N, R0 + t0 * utile, ka, nst)
+            Bj = _image_operand(dinv, s, ns, N, R0 + t1 * utile, ka, nst)
+            full = Ai @ Bj.T
+            a0, b0 = ri - (R0 + t0 * utile), rj - (R0 + t1 * utile)
+            img_upd = full[a0:a0 + ni, b0:b0 + nj]
+            assert np.allclose(img_upd, upd, rtol=1e-12,
+                               atol=1e-12 * max(1.0, np.abs(upd).max())), \
+                "tensor-core update operands differ from the factor rows"
+            upd = img_upd
+            if t0 == t1:
+                # diagonal tiles: the lower triangle only
+                upd = np.where(np.arange(ri, ri + ni)[:, None]
+                               >= np.arange(rj, rj + nj)[None, :], upd, 0.0)
+        F[ri:ri + ni, rj:rj + nj] -= upd
         if t0 == 0 and t1 == 0 and base < ns:
             _factor_diag(S, F, s, base, min(PANEL, ns - base), dinv)
     elif kind == PINV:
@@ -180,6 +270,11 @@ def replay_factor(sym, S, vals, dtype=0):
             dinv[("ltmp", s)] = np.full((S.ns(s), S.ns(s)), np.nan)
     utile = UTILE if dtype == 0 else 128
     bpan = 1 if dtype == 0 else 4
+    if dtype == 1:
+        off, total = image_offsets(S)
+        dinv[("img", 0)] = np.zeros(total)
+        for (s, q), o in off.items():
+            dinv[("imgoff", s, q)] = o
 
     def snapshot(d):
         return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
@@ -201,13 +296,16 @@ def replay_factor(sym, S, vals, dtype=0):
             assert fwd_dinv.keys() == dinv.keys()
             for key, v in dinv.items():
                 u = fwd_dinv[key]
+                if not isinstance(v, np.ndarray):
+                    assert u == v
+                    continue
                 assert np.array_equal(np.isnan(u), np.isnan(v))
                 ok = ~np.isnan(u)
                 assert np.abs(u[ok] - v[ok]).max(initial=0.0) <= 1e-9 * max(
                     1.0, np.abs(u[ok]).max(initial=0.0)), \
                     f"launch kind {kind}: {key} depends on task order"
     npanels = sum((S.ns(s) + PANEL - 1) // PANEL for s in range(S.nsuper))
-    assert len([k for k in dinv if k[0] not in ("linv", "ltmp")]) == npanels, \
+    assert len([k for k in dinv if k[0] not in ("linv", "ltmp", "img", "imgoff")]) == npanels, \
         "a panel inverse was never stored"
     for s in range(S.nsuper):
         if S.ns(s) >= min_ns:
