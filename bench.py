@@ -59,6 +59,11 @@ WORKLOADS = {
                             "(x1.3), 21 electrodes, dipole-dipole n=1..6, nky 11",
                        l2="L2 flushed between timed steps (working set ~0.1 GB)",
                        flush=True),
+    "dc2d_batch": dict(desc="64 independent 2.5-D DC surveys of uneven size (5k-40k "
+                            "cells, 24-64 electrodes, dipole-dipole n=1..6, nky 12) "
+                            "in the same launches; autotuned schedule shapes",
+                       l2="inputs larger than L2 (float32 fronts of 64 surveys)",
+                       flush=False),
     # a reduced 3-D case for profiler captures (a few GB on the device)
     "dc3d_mid": dict(desc="3-D DC, TensorMesh 40x40x20 core @8 m + 6 padding/face "
                           "(x1.3), same 200 sources and 6,000 data",
@@ -90,6 +95,10 @@ def build_case(name, seed):
         return syn.dc3d(seed=seed, ncore=(40, 40, 20), dx=8.0, npad=6)
     if name == "dc2d_large":
         return syn.dc2d_large(seed=seed)
+    if name == "dc2d_batch":
+        probs = syn.dc2d_batch(n_problems=64, seed=seed)
+        return ([(mesh, survey) for mesh, survey, _ in probs], None,
+                np.concatenate([m for *_, m in probs]))
     return syn.dc2d_small(seed=seed)
 
 
@@ -100,7 +109,13 @@ def workload_config(name):
 
 
 def make_engine(name, mesh, survey, device, dtype):
-    from simpeg_dc_torch_b200 import TorchDC2D, TorchDC3D
+    """The engine of a workload; for dc2d_batch `mesh` is the list of
+    (mesh, survey) problems."""
+    from simpeg_dc_torch_b200 import TorchDC2D, TorchDC2DBatch, TorchDC3D
+    if name == "dc2d_batch":
+        import torch
+        return TorchDC2DBatch(mesh, nky=12, device=device, dtype=dtype,
+                              tune=dtype == torch.float32)
     if name in ("dc3d", "dc3d_mid"):
         return TorchDC3D(mesh, survey, device=device, dtype=dtype)
     nky = 12 if name == "dc2d_large" else 11
@@ -203,6 +218,9 @@ class ReferenceCpu:
         from oracle import dc_oracle as O
         from simpeg_dc_torch_b200 import synthetic as syn
         self.name, self.O = name, O
+        if name == "dc2d_batch":
+            self._init_batch(seed)
+            return
         mesh, survey, m = build_case(name, seed)
         self.op = op = oracle_ops(name, mesh, survey)
         self.m = m
@@ -240,8 +258,52 @@ class ReferenceCpu:
                      f"{self.nS} columns each way) plus the projection / "
                      f"contraction rest timed once ({self.t_rest:.0f} ms)")
 
+    def _init_batch(self, seed):
+        """dc2d_batch: every survey with its own operators and quadrature;
+        step k factors and solves wavenumber system k of every survey
+        (forward and adjoint, all its sources) and scales by the number of
+        systems: over a cycle of steps, exactly the factorizations and
+        solves of one eval+grad of all 64 surveys (the projection /
+        contraction rest is left out, so the CPU time is understated)."""
+        import scipy.sparse as sp
+        from simpeg_dc_torch_b200.quadrature import (electrode_distance_range,
+                                                     k0_quadrature)
+        from simpeg_dc_torch_b200.operators import nodal_operators
+        problems, _, m = build_case("dc2d_batch", seed)
+        self.surveys = []
+        c0 = 0
+        for mesh, survey in problems:
+            o = nodal_operators(mesh, survey)
+            kys, wq, _ = k0_quadrature(*electrode_distance_range(survey), 12)
+            mb = m[c0:c0 + o.nC]
+            c0 += o.nC
+            sig = np.exp(-mb)
+            vals = [o.L_ky(k) @ sig for k in kys]
+            self.surveys.append((o, vals))
+        self.nky = max(len(v) for _, v in self.surveys)
+        self.step_i = 0
+        self.desc = ("each step: SuperLU factorization of wavenumber system k of "
+                     "all 64 surveys and their forward + adjoint solves (all "
+                     "sources), scaled by the number of systems (projection / "
+                     "contraction left out)")
+
     def step(self):
-        O, op = self.O, self.op
+        O = self.O
+        if self.name == "dc2d_batch":
+            import scipy.sparse as sp
+            import scipy.sparse.linalg as spla
+            k = self.step_i % self.nky
+            self.step_i += 1
+            t = time.perf_counter()
+            for o, vals in self.surveys:
+                if k >= len(vals):
+                    continue
+                lu = spla.splu(sp.csr_matrix((vals[k], o.col, o.crow),
+                                             shape=(o.nN, o.nN)).tocsc())
+                x = lu.solve(o.q.toarray())
+                lu.solve(np.ascontiguousarray(x[::-1]))
+            return 1e3 * self.nky * (time.perf_counter() - t)
+        op = self.op
         if self.name == "dc2d_small":
             t = time.perf_counter()
             O.misfit_grad_2d(op, self.m, self.dobs, self.w)
@@ -362,7 +424,7 @@ def cpu_baseline_leg(name):
     ref.step()
     t0 = time.perf_counter()
     ts = []
-    while len(ts) < 3 or (len(ts) < 10 and time.perf_counter() - t0 < 20):
+    while len(ts) < 3 or (len(ts) < 12 and time.perf_counter() - t0 < 30):
         ts.append(ref.step())
     return {"value": float(np.mean(ts)), "unit": "ms", "cores": 1,
             "kind": "port", "sample": ref.desc,

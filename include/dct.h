@@ -96,6 +96,39 @@ int dct_symbolic_get_schedule(const dct_symbolic* sym, int32_t dtype,
  * CuDSSBatchSolver.__init__ (dctorch/solver.py:187-213). */
 int dct_plan_create(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
                     int32_t dtype, int32_t device, dct_plan** out);
+
+/* Schedule shapes a plan is built with (the front tiles of its launches);
+ * dct_tuning_default fills the measured defaults of the dtype.  Any field
+ * <= 0 takes its default.
+ *   small_front_max   largest front factored by one CTA in shared memory
+ *                     (32 .. 224 float32, 32 .. 160 float64); larger fronts
+ *                     take the panel / trailing-update path
+ *   update_block      panels per block of the float32 trailing update (1..4;
+ *                     the deferred update after a block has K = 64 x this)
+ *   solve_target      float32 substitution: fewest tasks a launch is split
+ *                     into (K ranges halved until reached)
+ *   solve_split_max   float32 substitution: longest K piece of one task
+ *   solve_split_min   float32 substitution: shortest K piece
+ *   small_tc          single-panel supernodes on the tensor-core products:
+ *                     1 yes, 2 no (CUDA-core one-CTA kernels), <= 0 decided
+ *                     from where their work lies
+ * The tuner of the Python package (simpeg_dc_torch_b200/tuning.py) times
+ * candidate plans and keeps the fastest.  No counterpart in the reference:
+ * cuDSS chooses its own (dctorch/solver.py:103-109). */
+typedef struct {
+  int32_t small_front_max;
+  int32_t update_block;
+  int32_t solve_target;
+  int32_t solve_split_max;
+  int32_t solve_split_min;
+  int32_t small_tc;
+} dct_tuning;
+int dct_tuning_default(int32_t dtype, dct_tuning* out);
+int dct_plan_create_tuned(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
+                          int32_t dtype, int32_t device, const dct_tuning* tuning,
+                          dct_plan** out);
+/* the tuning a plan was built with (defaults resolved) */
+int dct_plan_get_tuning(const dct_plan* plan, dct_tuning* out);
 void dct_plan_destroy(dct_plan* plan);
 /* Iterative refinement of float32 plans (no effect on float64 plans):
  * at most `iterations` corrections (default 2, at most 64) after the first

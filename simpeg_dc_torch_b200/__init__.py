@@ -7,7 +7,8 @@ reference's solver and engine interfaces:
     make_solver, make_batch_solver, DCTSolver, DCTBatchSolver,
     sparse_solve, sparse_solve_batch, sparse_solve_batch_prefactored,
     TorchDC2D, TorchDC3D, Linearization2D,
-    TorchIP2D, TorchIP3D (linearized IP), TorchDCIP2D (joint DC + IP)
+    TorchIP2D, TorchIP3D (linearized IP), TorchDCIP2D (joint DC + IP),
+    TorchDC2DBatch (many uneven 2.5-D surveys in the same launches)
 
 Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
 discretize / SimPEG objects.  The engines also take a discretize
@@ -27,3 +28,4 @@ from .simulation2d import Linearization2D, TorchDC2D  # noqa: F401
 from .simulation3d import TorchDC3D  # noqa: F401
 from .ip import TorchIP2D, TorchIP3D  # noqa: F401
 from .dcip import TorchDCIP2D  # noqa: F401
+from .batch import TorchDC2DBatch  # noqa: F401

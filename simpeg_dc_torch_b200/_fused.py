@@ -48,7 +48,7 @@ class FusedPath:
 
     def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
                  coords=None, refine=None, n_rhs=None, refine_fields=None,
-                 refine_tol=None):
+                 refine_tol=None, tuning=None):
         self.device = device
         nN = crow.size - 1
         self.nN, self.nnzA = nN, col.size
@@ -61,7 +61,8 @@ class FusedPath:
         self._pri = None      # singularity-removal split (set_primary)
         self.solver = DCTBatchSolver(crow, col, nN, self.width, self.nbatch,
                                      device=device, dtype=dt, coords=coords,
-                                     refine=refine, refine_tol=refine_tol)
+                                     refine=refine, refine_tol=refine_tol,
+                                     tuning=tuning)
         plan = self.solver.plan
         self._plan = plan
         # float32 plans: most refinement corrections of the forward and of

@@ -52,6 +52,16 @@ class SymbolicInfo(C.Structure):
                 ("flops_factor", C.c_double)]
 
 
+class Tuning(C.Structure):
+    """dct_tuning: the schedule shapes of a plan (0 = default)."""
+    _fields_ = [("small_front_max", _i32), ("update_block", _i32),
+                ("solve_target", _i32), ("solve_split_max", _i32),
+                ("solve_split_min", _i32), ("small_tc", _i32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 _SIGS = {
     "dct_version": (C.c_int, []),
     "dct_last_error": (C.c_char_p, []),
@@ -63,6 +73,10 @@ _SIGS = {
     "dct_symbolic_get_schedule": (C.c_int, [_p, _i32, _i32, _p, _pi64, _p,
                                             _pi64]),
     "dct_plan_create": (C.c_int, [_p, _i32, _i32, _i32, _i32, C.POINTER(_p)]),
+    "dct_plan_create_tuned": (C.c_int, [_p, _i32, _i32, _i32, _i32,
+                                        C.POINTER(Tuning), C.POINTER(_p)]),
+    "dct_tuning_default": (C.c_int, [_i32, C.POINTER(Tuning)]),
+    "dct_plan_get_tuning": (C.c_int, [_p, C.POINTER(Tuning)]),
     "dct_plan_destroy": (None, [_p]),
     "dct_plan_set_refinement": (C.c_int, [_p, _i32]),
     "dct_plan_set_refinement_tolerance": (C.c_int, [_p, C.c_double]),
@@ -200,11 +214,16 @@ class Symbolic:
 class Plan:
     """Numeric plan: nbatch systems on the pattern of `sym`, on one device."""
 
-    def __init__(self, sym: Symbolic, nbatch, max_rhs, dtype, device):
+    def __init__(self, sym: Symbolic, nbatch, max_rhs, dtype, device, tuning=None):
         h = _p()
-        check(lib().dct_plan_create(sym.handle, int(nbatch), int(max_rhs),
-                                    int(dtype), int(device), C.byref(h)),
-              "dct_plan_create")
+        tu = None
+        if tuning is not None:
+            tu = Tuning(**{k: int(v) for k, v in dict(tuning).items()})
+        check(lib().dct_plan_create_tuned(sym.handle, int(nbatch), int(max_rhs),
+                                          int(dtype), int(device),
+                                          None if tu is None else C.byref(tu),
+                                          C.byref(h)),
+              "dct_plan_create_tuned")
         self._h = h
         self.sym = sym
         self.nbatch, self.max_rhs, self.dtype = int(nbatch), int(max_rhs), dtype
@@ -216,6 +235,12 @@ class Plan:
     @property
     def handle(self):
         return self._h
+
+    def tuning(self):
+        """The schedule shapes this plan was built with."""
+        t = Tuning()
+        check(lib().dct_plan_get_tuning(self._h, C.byref(t)), "dct_plan_get_tuning")
+        return t.as_dict()
 
     def set_refinement(self, iters):
         check(lib().dct_plan_set_refinement(self._h, int(iters)),
@@ -301,3 +326,9 @@ class Plan:
 
     def __del__(self):
         self.free()
+
+
+def default_tuning(dtype):
+    t = Tuning()
+    check(lib().dct_tuning_default(int(dtype), C.byref(t)), "dct_tuning_default")
+    return t.as_dict()

@@ -169,6 +169,36 @@ constexpr int kTcSplitK = DCT_TC_SPLITK;
 constexpr int kTcTargetCtas = DCT_TC_TARGET_CTAS;
 constexpr int kTcSplitMin = DCT_TC_SPLIT_MIN;
 
+// The measured defaults of the schedule shapes (see dct_tuning in dct.h),
+// and a user tuning with its zero fields defaulted and the rest clamped to
+// what the kernels support.
+dct_tuning default_tuning(int dtype) {
+  dct_tuning t;
+  t.small_front_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
+  t.update_block = dtype == DCT_F64 ? 1 : dct::kUpdateBlockPanels;
+  t.solve_target = kTcTargetCtas;
+  t.solve_split_max = kTcSplitK;
+  t.solve_split_min = kTcSplitMin;
+  t.small_tc = 0;
+  return t;
+}
+
+dct_tuning resolve_tuning(int dtype, const dct_tuning* in) {
+  dct_tuning t = default_tuning(dtype);
+  if (in == nullptr) return t;
+  const int smax = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
+  if (in->small_front_max > 0) t.small_front_max = std::max(32, std::min(smax, in->small_front_max));
+  // float64 fronts update after every panel (no blocking)
+  if (in->update_block > 0 && dtype == DCT_F32) t.update_block = std::min(4, in->update_block);
+  if (in->solve_target > 0) t.solve_target = in->solve_target;
+  if (in->solve_split_max > 0) t.solve_split_max = std::max(16, in->solve_split_max);
+  if (in->solve_split_min > 0) t.solve_split_min = std::max(16, in->solve_split_min);
+  t.solve_split_min = std::min(t.solve_split_min, t.solve_split_max);
+  if (in->small_tc > 0) t.small_tc = std::min(2, in->small_tc);
+  return t;
+}
+
+
 void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
   sc->flops.assign(sc->launches.size(), 0.0);
   sc->bytes.assign(sc->launches.size(), 0.0);
@@ -228,10 +258,6 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
 // trailing-update tile: 64 for float64 (CUDA cores), 128 for float32
 // (tcgen05 tensor-core tiles, M = N = 128)
 int update_tile(int dtype) { return dtype == DCT_F64 ? dct::kUpdateTile : 128; }
-// panels per block of the trailing update (dct::update_range): float32
-// fronts defer the update of the columns beyond the block and apply it with
-// K = up to 4 panels; float64 fronts update after every panel
-int update_block(int dtype) { return dtype == DCT_F64 ? 1 : dct::kUpdateBlockPanels; }
 
 void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int bpan,
                            bool align8, dct::Schedule* out) {
@@ -322,8 +348,8 @@ void push_split(std::vector<PanelTask>& T, int s, int t, int k0, int k1, int spl
   for (int a = k0; a < k1; a += split) T.push_back({s, a, t, std::min(k1, a + split)});
 }
 
-void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd,
-                           dct::Schedule* bwd) {
+void build_solve_schedules(const dct::Symbolic& S, int dtype, const dct_tuning& tu,
+                           dct::Schedule* fwd, dct::Schedule* bwd) {
   const bool tc = dtype == DCT_F32;
   // Single-panel supernodes run in one CTA each (k_fwd_small / k_bwd_small),
   // except in float32 plans whose single-panel fronts are mostly large (at
@@ -333,7 +359,9 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
   // tensor-core task costs more than it saves.
   constexpr int kTcSmallFront = 128;
   bool small_tc = false;
-  if (tc) {
+  if (tc && tu.small_tc == 1) {
+    small_tc = true;
+  } else if (tc && tu.small_tc != 2) {
     double big = 0, all = 0;
     for (int s = 0; s < S.nsuper; ++s) {
       const double ns = S.ns(s), nb = S.nb(s);
@@ -345,14 +373,15 @@ void build_solve_schedules(const dct::Symbolic& S, int dtype, dct::Schedule* fwd
     small_tc = all > 0 && big >= 0.5 * all;
   }
   auto is_small = [&](int s) { return S.ns(s) <= dct::kPanel && !small_tc; };
-  int split = kTcSplitK;   // K piece of the tensor-core tasks being filled
+  int split = tu.solve_split_max;   // K piece of the tensor-core tasks being filled
   std::vector<PanelTask> tmp;
   auto add = [&](dct::Schedule* sc, int kind, int lv, auto&& fill) {
     Launch l{kind, lv, int64_t(sc->tasks.size()), 0, 0};
-    for (split = kTcSplitK;; split /= 2) {
+    for (split = tu.solve_split_max;; split /= 2) {
       tmp.clear();
       fill(tmp);
-      if (!tc || int64_t(tmp.size()) >= kTcTargetCtas || split / 2 < kTcSplitMin) break;
+      if (!tc || int64_t(tmp.size()) >= tu.solve_target || split / 2 < tu.solve_split_min)
+        break;
     }
     sc->tasks.insert(sc->tasks.end(), tmp.begin(), tmp.end());
     l.count = int64_t(sc->tasks.size()) - l.first;
@@ -664,10 +693,11 @@ int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t whic
       (dtype != DCT_F64 && dtype != DCT_F32))
     return fail(DCT_ERR_ARG, "bad arguments");
   dct::Schedule f, fw, bw, iv;
-  const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(h->sym, small_max, update_tile(dtype), update_block(dtype),
+  const dct_tuning tu = default_tuning(dtype);
+  const int small_max = tu.small_front_max;
+  build_factor_schedule(h->sym, small_max, update_tile(dtype), tu.update_block,
                         dtype == DCT_F32, &f);
-  build_solve_schedules(h->sym, dtype, &fw, &bw);
+  build_solve_schedules(h->sym, dtype, tu, &fw, &bw);
   std::vector<int64_t> off;
   int64_t tot = 0;
   build_inverse_schedule(h->sym, small_max, &iv, &off, &tot);
@@ -713,8 +743,26 @@ void dct_plan_destroy(dct_plan* P) {
   delete P;
 }
 
+int dct_tuning_default(int32_t dtype, dct_tuning* out) {
+  if (!out || (dtype != DCT_F64 && dtype != DCT_F32)) return fail(DCT_ERR_ARG, "bad arguments");
+  *out = default_tuning(dtype);
+  return DCT_OK;
+}
+
+int dct_plan_get_tuning(const dct_plan* P, dct_tuning* out) {
+  if (!P || !out) return fail(DCT_ERR_ARG, "null argument");
+  *out = P->tune;
+  return DCT_OK;
+}
+
 int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
                     int32_t dtype, int32_t device, dct_plan** out) {
+  return dct_plan_create_tuned(h, nbatch, max_rhs, dtype, device, nullptr, out);
+}
+
+int dct_plan_create_tuned(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
+                          int32_t dtype, int32_t device, const dct_tuning* tuning,
+                          dct_plan** out) {
   if (!h || !out || nbatch < 1 || max_rhs < 1 ||
       (dtype != DCT_F64 && dtype != DCT_F32))
     return fail(DCT_ERR_ARG, "bad arguments");
@@ -747,11 +795,12 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
       (rc = upload(P, S.perm, &D.perm)) || (rc = upload(P, S.iperm, &D.iperm)) ||
       (rc = upload(P, S.in_crow, &D.crow)) || (rc = upload(P, S.in_col, &D.col)))
     return bail(rc);
-  const int small_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  build_factor_schedule(S, small_max, update_tile(dtype), update_block(dtype),
+  P->tune = resolve_tuning(dtype, tuning);
+  const int small_max = P->tune.small_front_max;
+  build_factor_schedule(S, small_max, update_tile(dtype), P->tune.update_block,
                         dtype == DCT_F32, &P->fact);
-  P->update_bpan = update_block(dtype);
-  build_solve_schedules(S, dtype, &P->fwd, &P->bwd);
+  P->update_bpan = P->tune.update_block;
+  build_solve_schedules(S, dtype, P->tune, &P->fwd, &P->bwd);
   std::vector<int64_t> dinv_off;
   build_inverse_schedule(S, small_max, &P->inv, &dinv_off, &P->dinv_stride);
   {
@@ -793,7 +842,7 @@ int dct_plan_create(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
     P->img = dct::ImgArgs{static_cast<float*>(img), d_off, d_pf, acc};
   }
   account_factor(S, &P->fact, double(esize(dtype)), update_tile(dtype),
-                 update_block(dtype), dtype == DCT_F32);
+                 P->update_bpan, dtype == DCT_F32);
   account_solve(S, &P->fwd, double(esize(dtype)));
   account_solve(S, &P->bwd, double(esize(dtype)));
   if ((rc = upload_schedule(P, &P->fact)) || (rc = upload_schedule(P, &P->fwd)) ||

@@ -244,6 +244,7 @@ struct dct_plan {
   int factored = 0;
   int64_t stamp = 0;
   dct::ImgArgs img{};              // f32 plans: split panel images (large fronts)
+  dct_tuning tune{};               // schedule shapes (resolved, no zero fields)
   int ir_iters = 2;                // most refinement iterations of f32 plans
   double ir_tol = 0.0;             // stop once the estimated error is below (0: fixed count)
   dct::IrState* ir = nullptr;      // device: refinement state of the last solve

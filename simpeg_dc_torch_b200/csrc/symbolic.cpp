@@ -74,6 +74,9 @@ class Dissector {
  private:
   bool split(const std::vector<int32_t>& nodes, std::vector<int32_t>& L,
              std::vector<int32_t>& R, std::vector<int32_t>& S) {
+    if (component_split(nodes, L, R)) return true;
+    L.clear();
+    R.clear();
     if (coords_ != nullptr && plane_split(nodes, L, R, S)) return true;
     L.clear();
     R.clear();
@@ -122,6 +125,51 @@ class Dissector {
       else S.push_back(v);
     }
     return !(L.empty() && R.empty());
+  }
+
+  // A disconnected subset (several independent systems assembled side by
+  // side, e.g. a batch of surveys) splits between its components with an
+  // empty separator: the components are dealt largest first to the lighter
+  // side, so the two halves carry about the same number of nodes.
+  bool component_split(const std::vector<int32_t>& nodes, std::vector<int32_t>& L,
+                       std::vector<int32_t>& R) {
+    ++stamp_;
+    for (int32_t v : nodes) mark_[v] = stamp_;
+    if (cmark_.empty()) cmark_.assign(g_.n, -1);
+    ++cstamp_;
+    std::vector<std::vector<int32_t>> comps;
+    for (int32_t v0 : nodes) {
+      if (cmark_[v0] == cstamp_) continue;
+      std::vector<int32_t> c{v0};
+      cmark_[v0] = cstamp_;
+      for (size_t h = 0; h < c.size(); ++h) {
+        const int32_t v = c[h];
+        for (int64_t p = g_.ptr[v]; p < g_.ptr[v + 1]; ++p) {
+          const int32_t u = g_.adj[p];
+          if (mark_[u] == stamp_ && cmark_[u] != cstamp_) {
+            cmark_[u] = cstamp_;
+            c.push_back(u);
+          }
+        }
+      }
+      if (comps.empty() && c.size() == nodes.size()) return false;   // connected
+      comps.push_back(std::move(c));
+    }
+    std::stable_sort(comps.begin(), comps.end(),
+                     [](const std::vector<int32_t>& x, const std::vector<int32_t>& y) {
+                       return x.size() > y.size();
+                     });
+    size_t nl = 0, nr = 0;
+    for (const auto& c : comps) {
+      if (nl <= nr) {
+        L.insert(L.end(), c.begin(), c.end());
+        nl += c.size();
+      } else {
+        R.insert(R.end(), c.begin(), c.end());
+        nr += c.size();
+      }
+    }
+    return true;
   }
 
   // breadth-first levels within the current subset; returns the depth
@@ -216,8 +264,8 @@ class Dissector {
   const Graph& g_;
   const int32_t* coords_;
   int ndim_, leaf_;
-  std::vector<int32_t> mark_, side_, seen_, levv_;
-  int stamp_ = 0, stamp2_ = 0;
+  std::vector<int32_t> mark_, side_, seen_, levv_, cmark_;
+  int stamp_ = 0, stamp2_ = 0, cstamp_ = 0;
   std::vector<NDNode> tree_;
 };
 

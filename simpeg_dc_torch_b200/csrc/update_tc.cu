@@ -7,14 +7,15 @@
 //   warp 0    one thread issues the bulk copies (cp.async.bulk ... complete_tx)
 //             of each K stage -- 32 columns of the hi and lo images of the
 //             tile's row block i and column block j, 16 KB each, contiguous in
-//             the images -- into a three-stage ring, each stage guarded by a
+//             the images -- into a two-stage ring, each stage guarded by a
 //             "full" mbarrier (transaction bytes) and an "empty" one;
 //   warp 1    allocates TMEM and one thread issues tcgen05.mma kind::tf32 for
 //             each stage (3xTF32: hi*hi + hi*lo + lo*hi; Markidis et al. 2018,
 //             Ootomo & Yokota 2022), then commits to the stage's "empty"
 //             barrier so the ring slot can be refilled;
-//   warps 2-5 wait for the last commit, read the accumulators from TMEM (one
-//             row per thread) and subtract them from the tile in place.
+//   warps 2-5 copy the output tile into shared memory (cp.async, one row
+//             per thread) while the MMAs run, wait for the last commit, read
+//             the accumulators from TMEM and store the difference.
 // No thread converts or stages operands: the split happens once per panel,
 // not once per tile and K stage.
 //
@@ -39,12 +40,13 @@ namespace dct {
 namespace {
 
 constexpr int kUThreads = 192;
-constexpr int kUStages = 3;
+constexpr int kUStages = 2;
 constexpr int kUChunk = 16384;              // 128 rows x 32 columns, hi or lo
 constexpr int kUStageBytes = 4 * kUChunk;   // A hi, A lo, B hi, B lo
 constexpr uint32_t kULbo = 128, kUSbo = 1024;
 constexpr int kUAcc = 4;                    // accumulators: one per panel
-constexpr size_t kUSmem = size_t(kUStages) * kUStageBytes + 128;
+constexpr int kUTileBytes = kTcM * kTcN * 4;   // the output tile, staged
+constexpr size_t kUSmem = size_t(kUStages) * kUStageBytes + kUTileBytes + 128;
 static_assert(kUAcc * 128 <= 512, "TMEM columns of one SM");
 static_assert(size_t(kUStages) * kUStageBytes >= sizeof(float) * kDiagSmemElems,
               "the ring also holds factor_diag's workspace");
@@ -87,7 +89,8 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   pdl_trigger();
   // the bulk copies and the MMA descriptors need 16-byte alignment
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kUStages * kUStageBytes);
+  float* Cs = reinterpret_cast<float*>(smem_raw + kUStages * kUStageBytes);   // [col][row]
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kUStages * kUStageBytes + kUTileBytes);
   uint64_t* empty = full + kUStages;
   uint64_t* done = empty + kUStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -201,27 +204,37 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
       umma_commit(done);
     }
   } else {
-    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile rows
+    // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 = tile rows.  The
+    // thread's row of the tile is copied into shared memory (cp.async)
+    // while the MMAs run, so its read latency hides behind the K loop.
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
+    const int row = ri + r;
+    const bool row_ok = row >= base && row < N;
+    // column c of the tile is written when in range and, in a diagonal
+    // tile, on or below the diagonal
+    const int c_lo = max(0, base - rj);
+    const int c_hi = row_ok ? min(jn, diag ? row - rj + 1 : jn) : 0;
+    const float* src = F + row + int64_t(rj) * N;
+    for (int c = c_lo; c < c_hi; ++c)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(Cs + c * kTcM + r)),
+                   "l"(src + int64_t(c) * N)
+                   : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
     bool got = false;
     if (lane == 0) got = mbar_wait1(done, 0);
     got = __shfl_sync(0xffffffffu, got ? 1 : 0, 0) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("cp.async.wait_all;" ::: "memory");
     if (!got) {
       ok = false;
       if (lane == 0) flag_timeout(status, s, b);
     } else {
-      const int quarter = warp & 3;
-      const int row = ri + quarter * 32 + lane;
-      const bool row_ok = row >= base && row < N;
-      float* dst = F + min(row, N - 1);
+      float* dst = F + min(row, N - 1) + int64_t(rj) * N;
       for (int cb = 0; cb < np; cb += 32) {
         float cur[32];
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int col = rj + cb + c;
-          const bool in = row_ok && cb + c < jn && col >= base && (!diag || col <= row);
-          cur[c] = in ? dst[int64_t(col) * N] : 0.0f;
-        }
+        for (int c = 0; c < 32; ++c) cur[c] = Cs[(cb + c) * kTcM + r];
         for (int a = 0; a < nacc; ++a) {
           uint32_t v[32];
           tmem_ld32(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(a * 128 + cb), v);
@@ -229,11 +242,8 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
           for (int c = 0; c < 32; ++c) cur[c] -= __uint_as_float(v[c]);
         }
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int col = rj + cb + c;
-          if (row_ok && cb + c < jn && col >= base && (!diag || col <= row))
-            dst[int64_t(col) * N] = cur[c];
-        }
+        for (int c = 0; c < 32; ++c)
+          if (cb + c >= c_lo && cb + c < c_hi) dst[int64_t(cb + c) * N] = cur[c];
       }
     }
   }

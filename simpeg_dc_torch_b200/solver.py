@@ -67,7 +67,8 @@ class _PlanSolver:
     """Shared machinery of the single and batched solvers."""
 
     def __init__(self, crow, col, n, n_rhs, nbatch, device, dtype,
-                 matrix_type, coords, refine, leaf_size, refine_tol=None):
+                 matrix_type, coords, refine, leaf_size, refine_tol=None,
+                 tuning=None):
         if matrix_type not in _MATRIX_TYPES:
             raise NotImplementedError(
                 f"matrix_type {matrix_type!r}: only real SPD systems are "
@@ -90,7 +91,7 @@ class _PlanSolver:
         self._sym = nat.Symbolic(crow_np, col_np, coords, leaf_size)
         with torch.cuda.device(self.device):
             self._plan = nat.Plan(self._sym, self.nbatch, self.n_rhs,
-                                  self._code, self.device.index)
+                                  self._code, self.device.index, tuning)
         # refinement of float32 plans: at most `refine` corrections (the
         # library default is 2), fewer once the estimated error is below
         # `refine_tol` (0, the library default: a fixed count)
@@ -170,9 +171,9 @@ class DCTSolver(_PlanSolver):
 
     def __init__(self, crow, col, n, n_rhs, device="cuda",
                  dtype=torch.float64, matrix_type="spd", coords=None,
-                 refine=None, leaf_size=64, refine_tol=None):
+                 refine=None, leaf_size=64, refine_tol=None, tuning=None):
         super().__init__(crow, col, n, n_rhs, 1, device, dtype, matrix_type,
-                         coords, refine, leaf_size, refine_tol)
+                         coords, refine, leaf_size, refine_tol, tuning)
 
     def factorize(self, values):
         """Numeric refactorization with new values (nnz,), same pattern."""
@@ -193,9 +194,9 @@ class DCTBatchSolver(_PlanSolver):
 
     def __init__(self, crow, col, n, n_rhs, nbatch, device="cuda",
                  dtype=torch.float64, matrix_type="spd", coords=None,
-                 refine=None, leaf_size=64, refine_tol=None):
+                 refine=None, leaf_size=64, refine_tol=None, tuning=None):
         super().__init__(crow, col, n, n_rhs, nbatch, device, dtype,
-                         matrix_type, coords, refine, leaf_size, refine_tol)
+                         matrix_type, coords, refine, leaf_size, refine_tol, tuning)
 
     def factorize(self, values):
         """values: (nbatch, nnz) -- refactorize every system."""

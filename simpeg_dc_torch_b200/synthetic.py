@@ -190,12 +190,13 @@ def dc2d_large(seed=0):
     return mesh, survey, m
 
 
-def dc2d_batch(n_problems=64, seed=0):
-    """List of (mesh, survey, m) of uneven size (5k-40k cells)."""
+def dc2d_batch(n_problems=64, seed=0, scale=1.0):
+    """List of (mesh, survey, m) of uneven size (5k-40k cells; `scale`
+    multiplies the cell counts, for small test batches)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(n_problems):
-        target = rng.uniform(5e3, 4e4)
+        target = rng.uniform(5e3, 4e4) * scale
         npad = 8
         ncy = int(np.sqrt(target / 3.0))
         ncx = max(int(target / (ncy + npad)) - 2 * npad, 40)
