@@ -48,7 +48,7 @@ class FusedPath:
 
     def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
                  coords=None, refine=None, n_rhs=None, refine_fields=None,
-                 refine_tol=None, tuning=None):
+                 refine_tol=None, tuning=None, leaf_size=64):
         self.device = device
         nN = crow.size - 1
         self.nN, self.nnzA = nN, col.size
@@ -62,7 +62,7 @@ class FusedPath:
         self.solver = DCTBatchSolver(crow, col, nN, self.width, self.nbatch,
                                      device=device, dtype=dt, coords=coords,
                                      refine=refine, refine_tol=refine_tol,
-                                     tuning=tuning)
+                                     tuning=tuning, leaf_size=leaf_size)
         plan = self.solver.plan
         self._plan = plan
         # float32 plans: most refinement corrections of the forward and of

@@ -79,7 +79,7 @@ class TorchDC2D:
                  dtype=torch.float64, active_cells=None, val_inactive=None,
                  chunk=None, singularity_removal=False, rho_primary=None,
                  quadrature=None, refine=None, refine_fields=None,
-                 refine_tol=None):
+                 refine_tol=None, leaf_size=64):
         if quadrature is None:
             quadrature = os.environ.get("DCTORCH_QUADRATURE", "electrodes")
         if isinstance(quadrature, str) and quadrature != "electrodes":
@@ -129,6 +129,7 @@ class TorchDC2D:
                                coords=mesh.node_grid_index()
                                if hasattr(mesh, "node_grid_index") else None,
                                refine=refine, refine_fields=refine_fields,
+                               leaf_size=leaf_size,
                                refine_tol=(1e-9 if refine_tol is None
                                            else refine_tol))
         self.solver = self._path.solver

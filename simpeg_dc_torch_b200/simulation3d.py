@@ -24,7 +24,8 @@ class TorchDC3D:
 
     def __init__(self, mesh, survey, device="cuda", dtype=torch.float64,
                  active_cells=None, val_inactive=None, bc_type="Robin",
-                 refine=None, refine_fields=None, refine_tol=None):
+                 refine=None, refine_fields=None, refine_tol=None,
+                 leaf_size=64):
         if bc_type != "Robin":
             raise NotImplementedError("only the Robin boundary condition is built")
         self.device = torch.device(device)
@@ -50,6 +51,7 @@ class TorchDC3D:
                                coords=mesh.node_grid_index()
                                if hasattr(mesh, "node_grid_index") else None,
                                refine=refine, refine_fields=refine_fields,
+                               leaf_size=leaf_size,
                                refine_tol=refine_tol)
         self.solver = self._path.solver
         self.sidx = torch.as_tensor(ops.sidx, device=self.device)

@@ -140,6 +140,24 @@ def test_active_cells_restrict_the_gradient(cuda):
     ja = ea.Jtvec(torch.tensor(m_full[act], device=cuda), v).cpu().numpy()
     assert ja.shape == (int(act.sum()),)
     assert rel(ja, jf[act]) < 1e-12
+    # against the oracle: the model on the active cells injected into the
+    # full mesh with the inactive value, the gradient restricted back
+    # (dctorch/simulation2d.py:122-134, 299-304)
+    op = _oracle_ops_2d(ea)
+    d_ref = O.dpred_2d(op, m_full)
+    dobs, w = syn.observed(d_ref, np.random.default_rng(6))
+    _, g_ref = O.misfit_grad_2d(op, m_full, dobs, w)
+    for dtype, td, tg in [(torch.float64, 1e-10, 1e-9), (torch.float32, 1e-6, 1e-5)]:
+        eng = ea if dtype == torch.float64 else TorchDC2D(
+            mesh, survey, nky=7, device=cuda, dtype=dtype, active_cells=act,
+            val_inactive=val)
+        ma = torch.tensor(m_full[act], device=cuda, requires_grad=True)
+        eng.misfit(ma, torch.tensor(dobs, device=cuda),
+                   torch.tensor(w, device=cuda)).backward()
+        with torch.no_grad():
+            d = eng.dpred(torch.tensor(m_full[act], device=cuda)).cpu().numpy()
+        assert rel(d, d_ref) < td
+        assert rel(ma.grad.cpu().numpy(), g_ref[act]) < tg
 
 
 def test_adjoint_survives_a_clobbered_factorization(cuda):
