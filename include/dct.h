@@ -26,7 +26,9 @@
 extern "C" {
 #endif
 
-enum { DCT_F64 = 0, DCT_F32 = 1 };
+/* value types: float64, float32, and complex128 (two doubles re, im; the
+ * complex-symmetric systems of the complex-resistivity engine) */
+enum { DCT_F64 = 0, DCT_F32 = 1, DCT_C128 = 2 };
 
 enum {
   DCT_OK = 0,
@@ -92,6 +94,12 @@ int dct_symbolic_get_schedule(const dct_symbolic* sym, int32_t dtype,
  * dtype DCT_F64: plain float64 factor and solve.
  * dtype DCT_F32: float32 factor and solve, with iterative refinement whose
  *                residual b - A x is formed in float64.
+ * dtype DCT_C128: complex-symmetric (A^T = A, not Hermitian) A = L L^T
+ *                without conjugation, complex128 values and right-hand
+ *                sides (dct_factorize / dct_solve with DCT_C128 buffers;
+ *                dct_solve_permuted is float64 only).  Replaces cuDSS's
+ *                "symmetric" matrix type (dctorch/solver.py:44-47,
+ *                377-380) behind the complex-resistivity engine.
  * Replaces CuDSSSolver.__init__ (dctorch/solver.py:88-114) and
  * CuDSSBatchSolver.__init__ (dctorch/solver.py:187-213). */
 int dct_plan_create(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
@@ -255,9 +263,10 @@ int dct_gather_contract(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
                         const double* d_Y, const double* d_X, double* d_gv,
                         void* stream);
 
-/* Same contraction in the user's row order and dtype, for the solver-level
- * autograd op: gv[b,e] = -sum_r Y[b,row_e,r] X[b,col_e,r]
- * (dctorch/solver.py:160-170, 268-276). */
+/* Same contraction in the user's row order and dtype (DCT_F64, DCT_F32 or
+ * DCT_C128, complex without conjugation), for the solver-level autograd op:
+ * gv[b,e] = -sum_r Y[b,row_e,r] X[b,col_e,r] (dctorch/solver.py:160-170,
+ * 268-276). */
 int dct_gather_contract_plain(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
                               const int32_t* d_row, const int32_t* d_col,
                               int32_t dtype, const void* d_Y, const void* d_X,

@@ -440,6 +440,78 @@ def dcip_misfit_grad_2d(op, m, eta_max, ip_scale, dc_state, dobs_dc, w_dc,
     return phi, np.concatenate([grad_rho, grad_eta])
 
 
+def cr_dpred_2d(op, m_rho, chg, ip_scale=1.0, dc_datum="magnitude",
+                return_fields=False):
+    """Complex-resistivity 2.5-D data (dctorch/cr2d.py:74-97): the complex
+    conductivity sigma* = sigma (1 - i m) with sigma = exp(-m_rho), complex
+    values VALS = Lstack sigma*, U_k = A_k^{-1} q on complex SuperLU
+    (complex-symmetric A_k), Ubar = sum_k wq_k U_k, V = (Pd Ubar)[i, sidx_i];
+    d_rho = |V| ("magnitude") or Re V ("real"), d_ip = ip_scale Im V / Re V.
+    Returns (d_rho, d_ip) or, with return_fields, also (V, sigma*, lu, U)."""
+    nky = len(op["wq"])
+    sig = sigma_of(m_rho)
+    sstar = sig * (1.0 - 1j * np.asarray(chg, float))
+    L = op["Lstack"]
+    VALS = (L @ sstar.real + 1j * (L @ sstar.imag)).reshape(nky, -1)
+    n = op["nN"]
+    lu = [spla.splu(sp.csr_matrix((v, op["col"], op["crow"]), shape=(n, n)).tocsc())
+          for v in VALS]
+    Q = np.asarray(op["Q"], complex)
+    U = np.stack([f.solve(Q) for f in lu])
+    Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
+    PU = op["Pd"] @ Ubar
+    V = PU[np.arange(PU.shape[0]), op["sidx"]]
+    d_rho = np.abs(V) if dc_datum == "magnitude" else V.real.copy()
+    d_ip = ip_scale * V.imag / V.real
+    if return_fields:
+        return d_rho, d_ip, (V, sstar, lu, U)
+    return d_rho, d_ip
+
+
+def cr_misfit_grad_2d(op, m, ip_scale, dc_datum, dobs_rho, w_rho, dobs_ip, w_ip,
+                      lam):
+    """(phi, dphi/dm) of the complex-resistivity misfit (dctorch/cr2d.py:
+    104-108) for the stacked model m = cat(log-rho, chargeability).
+
+    V is holomorphic in sigma*, so for the real loss dphi = Re(G dV) with
+    G = dphi/dRe V - i dphi/dIm V.  The adjoint fields Y_k = A_k^{-1} Pd^T G
+    (complex, A_k^T = A_k) give h = Lstack^T gv, gv_k[e] = -wq_k sum_s
+    Y_k[row_e, s] U_k[col_e, s]; with dsigma* = -sigma* dm_rho - i sigma dm,
+    dphi/dm_rho = Re(-sigma* h) and dphi/dm = sigma Im(h)."""
+    m = np.asarray(m, float)
+    n = m.size // 2
+    m_rho, chg = m[:n], m[n:]
+    d_rho, d_ip, (V, sstar, lu, U) = cr_dpred_2d(op, m_rho, chg, ip_scale,
+                                                 dc_datum, return_fields=True)
+    r_rho = w_rho * (d_rho - dobs_rho)
+    r_ip = w_ip * (d_ip - dobs_ip)
+    phi = float((r_rho ** 2).sum() + lam * (r_ip ** 2).sum())
+    g_rho = 2.0 * w_rho * r_rho
+    g_ip = 2.0 * lam * w_ip * r_ip
+    Vr, Vi = V.real, V.imag
+    if dc_datum == "magnitude":
+        a = np.abs(V)
+        gr, gi = g_rho * Vr / a, g_rho * Vi / a
+    else:
+        gr, gi = g_rho.copy(), np.zeros_like(g_rho)
+    gr = gr - g_ip * ip_scale * Vi / Vr ** 2
+    gi = gi + g_ip * ip_scale / Vr
+    G = np.zeros((op["Pd"].shape[0], op["Q"].shape[1]), complex)
+    G[np.arange(G.shape[0]), op["sidx"]] = gr - 1j * gi
+    R = op["Pd"].T @ G
+    r = row_of(op["crow"])
+    nky = len(op["wq"])
+    gv = np.empty((nky, len(op["col"])), complex)
+    for k in range(nky):
+        Y = lu[k].solve(R)
+        gv[k] = -op["wq"][k] * np.einsum("es,es->e", Y[r], U[k][op["col"]])
+    L = op["Lstack"]
+    gvf = gv.reshape(-1)
+    h = L.T @ gvf.real + 1j * (L.T @ gvf.imag)
+    sig = sstar.real
+    return phi, np.concatenate([np.real(-sstar * h), sig * h.imag])
+
+
 def unit_primary_2d(nodes, kys, poles, radii):
     """Unit-resistivity half-space primary (dctorch/singularity.py:47-82):
     K_0(ky r) / pi summed over each source's poles (location, sign), and at

@@ -8,6 +8,7 @@ reference's solver and engine interfaces:
     sparse_solve, sparse_solve_batch, sparse_solve_batch_prefactored,
     TorchDC2D, TorchDC3D, Linearization2D,
     TorchIP2D, TorchIP3D (linearized IP), TorchDCIP2D (joint DC + IP),
+    TorchCR2D (complex resistivity, complex-symmetric systems),
     TorchDC2DBatch (many uneven 2.5-D surveys in the same launches)
 
 Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
@@ -28,4 +29,5 @@ from .simulation2d import Linearization2D, TorchDC2D  # noqa: F401
 from .simulation3d import TorchDC3D  # noqa: F401
 from .ip import TorchIP2D, TorchIP3D  # noqa: F401
 from .dcip import TorchDCIP2D  # noqa: F401
+from .cr2d import TorchCR2D  # noqa: F401
 from .batch import TorchDC2DBatch  # noqa: F401

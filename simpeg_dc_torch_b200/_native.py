@@ -15,7 +15,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libdct.so")
 
-F64, F32 = 0, 1
+F64, F32, C128 = 0, 1, 2
 
 STATUS = {
     0: "OK", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",

@@ -172,10 +172,16 @@ constexpr int kTcSplitMin = DCT_TC_SPLIT_MIN;
 // The measured defaults of the schedule shapes (see dct_tuning in dct.h),
 // and a user tuning with its zero fields defaulted and the rest clamped to
 // what the kernels support.
+// largest front the single-CTA kernel holds in shared memory (N^2 values)
+int small_front_limit(int dtype) {
+  return dtype == DCT_F64 ? dct::kSmallFrontF64
+                          : (dtype == DCT_C128 ? dct::kSmallFrontC128 : dct::kSmallFrontF32);
+}
+
 dct_tuning default_tuning(int dtype) {
   dct_tuning t;
-  t.small_front_max = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
-  t.update_block = dtype == DCT_F64 ? 1 : dct::kUpdateBlockPanels;
+  t.small_front_max = small_front_limit(dtype);
+  t.update_block = dtype == DCT_F32 ? dct::kUpdateBlockPanels : 1;
   t.solve_target = kTcTargetCtas;
   t.solve_split_max = kTcSplitK;
   t.solve_split_min = kTcSplitMin;
@@ -186,7 +192,7 @@ dct_tuning default_tuning(int dtype) {
 dct_tuning resolve_tuning(int dtype, const dct_tuning* in) {
   dct_tuning t = default_tuning(dtype);
   if (in == nullptr) return t;
-  const int smax = dtype == DCT_F64 ? dct::kSmallFrontF64 : dct::kSmallFrontF32;
+  const int smax = small_front_limit(dtype);
   if (in->small_front_max > 0) t.small_front_max = std::max(32, std::min(smax, in->small_front_max));
   // float64 fronts update after every panel (no blocking)
   if (in->update_block > 0 && dtype == DCT_F32) t.update_block = std::min(4, in->update_block);
@@ -257,7 +263,7 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
 
 // trailing-update tile: 64 for float64 (CUDA cores), 128 for float32
 // (tcgen05 tensor-core tiles, M = N = 128)
-int update_tile(int dtype) { return dtype == DCT_F64 ? dct::kUpdateTile : 128; }
+int update_tile(int dtype) { return dtype == DCT_F32 ? 128 : dct::kUpdateTile; }
 
 void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int bpan,
                            bool align8, dct::Schedule* out) {
@@ -531,7 +537,8 @@ int upload_schedule(dct_plan* P, dct::Schedule* sch) {
   return rc;
 }
 
-size_t esize(int dtype) { return dtype == DCT_F64 ? 8 : 4; }
+size_t esize(int dtype) { return dtype == DCT_F64 ? 8 : (dtype == DCT_C128 ? 16 : 4); }
+bool valid_dtype(int dtype) { return dtype == DCT_F64 || dtype == DCT_F32 || dtype == DCT_C128; }
 
 int set_device(int device) {
   int cur = -1;
@@ -689,8 +696,7 @@ int dct_symbolic_get_array(const dct_symbolic* h, const char* name, void* dst,
 int dct_symbolic_get_schedule(const dct_symbolic* h, int32_t dtype, int32_t which,
                               int32_t* tasks, int64_t* ntasks, int64_t* launches,
                               int64_t* nlaunches) {
-  if (!h || !ntasks || !nlaunches || which < 0 || which > 4 ||
-      (dtype != DCT_F64 && dtype != DCT_F32))
+  if (!h || !ntasks || !nlaunches || which < 0 || which > 4 || !valid_dtype(dtype))
     return fail(DCT_ERR_ARG, "bad arguments");
   dct::Schedule f, fw, bw, iv;
   const dct_tuning tu = default_tuning(dtype);
@@ -744,7 +750,7 @@ void dct_plan_destroy(dct_plan* P) {
 }
 
 int dct_tuning_default(int32_t dtype, dct_tuning* out) {
-  if (!out || (dtype != DCT_F64 && dtype != DCT_F32)) return fail(DCT_ERR_ARG, "bad arguments");
+  if (!out || !valid_dtype(dtype)) return fail(DCT_ERR_ARG, "bad arguments");
   *out = default_tuning(dtype);
   return DCT_OK;
 }
@@ -764,7 +770,7 @@ int dct_plan_create_tuned(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs
                           int32_t dtype, int32_t device, const dct_tuning* tuning,
                           dct_plan** out) {
   if (!h || !out || nbatch < 1 || max_rhs < 1 ||
-      (dtype != DCT_F64 && dtype != DCT_F32))
+      !valid_dtype(dtype))
     return fail(DCT_ERR_ARG, "bad arguments");
   *out = nullptr;
   int ndev = 0;
@@ -929,8 +935,9 @@ int64_t dct_plan_stamp(const dct_plan* P) { return P ? P->stamp : -1; }
 
 int dct_factorize(dct_plan* P, const void* d_vals, int32_t vals_dtype,
                   int64_t vals_batch_stride, void* stream) {
-  if (!P || !d_vals || (vals_dtype != DCT_F64 && vals_dtype != DCT_F32))
-    return fail(DCT_ERR_ARG, "bad arguments");
+  if (!P || !d_vals || !valid_dtype(vals_dtype) ||
+      ((vals_dtype == DCT_C128) != (P->dtype == DCT_C128)))
+    return fail(DCT_ERR_ARG, "bad arguments (complex values need a complex plan and back)");
   int rc = set_device(P->device);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -982,6 +989,8 @@ int dct_solve_permuted(dct_plan* P, const double* d_bp, int32_t b_batched,
   if (!P || !d_bp || !d_xp || k < 1 || k > P->max_rhs)
     return fail(DCT_ERR_ARG, "bad arguments");
   if (!P->factored) return fail(DCT_ERR_NOT_FACTORED, "solve before factorize");
+  if (P->dtype == DCT_C128)
+    return fail(DCT_ERR_ARG, "dct_solve_permuted takes float64 plans; use dct_solve");
   if (P->dtype == DCT_F32 && d_bp == d_xp)
     return fail(DCT_ERR_ARG, "float32 plans refine against the right-hand side: "
                              "d_bp must not alias d_xp");
@@ -1003,8 +1012,8 @@ int dct_solve_permuted(dct_plan* P, const double* d_bp, int32_t b_batched,
 
 int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
               int32_t k, void* d_x, void* stream) {
-  if (!P || !d_b || !d_x || k < 1 || k > P->max_rhs ||
-      (io_dtype != DCT_F64 && io_dtype != DCT_F32))
+  if (!P || !d_b || !d_x || k < 1 || k > P->max_rhs || !valid_dtype(io_dtype) ||
+      ((io_dtype == DCT_C128) != (P->dtype == DCT_C128)))
     return fail(DCT_ERR_ARG, "bad arguments");
   if (!P->factored) return fail(DCT_ERR_NOT_FACTORED, "solve before factorize");
   int rc = set_device(P->device);
@@ -1013,6 +1022,17 @@ int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
   const int n = P->sym.n;
   const int64_t per = int64_t(n) * k;
   const int64_t bstride = b_batched ? per : 0;
+  if (P->dtype == DCT_C128) {
+    DCT_CUDA(dct::launch_perm_in_any(d_b, DCT_C128, bstride, P->ds.perm, n, k,
+                                     P->nbatch, P->bufA, DCT_C128, st),
+             "permute rhs");
+    DCT_CUDA(dct::run_solve_c128(P, static_cast<dct::cplx*>(P->bufA), k, st),
+             "solve launch");
+    DCT_CUDA(dct::launch_perm_out_any(P->bufA, DCT_C128, P->ds.perm, n, k,
+                                      P->nbatch, d_x, DCT_C128, st),
+             "permute solution");
+    return DCT_OK;
+  }
   if (P->dtype == DCT_F64) {
     DCT_CUDA(dct::launch_perm_in_any(d_b, io_dtype, bstride, P->ds.perm, n, k,
                                      P->nbatch, P->bufA, DCT_F64, st),

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "../../include/dct.h"
+#include "cplx.cuh"
 #include "symbolic.h"
 
 namespace dct {
@@ -85,6 +86,7 @@ enum LaunchKind : int {
 // Limits of the single-CTA front kernel (front fully in shared memory).
 constexpr int kSmallFrontF64 = 160;
 constexpr int kSmallFrontF32 = 224;
+constexpr int kSmallFrontC128 = 112;
 constexpr int kThreads = 256;
 constexpr int kRhsChunk = 64;   // right-hand sides per CTA in the solves
 constexpr int kUpdateTile = 64;   // trailing-update tile (rows = cols)
@@ -290,6 +292,8 @@ cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,
                        int64_t vals_stride, cudaStream_t st);
 cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st);
 cudaError_t run_solve_f32(dct_plan* P, int k, cudaStream_t st);
+// complex128 plans: the permuted right-hand side in xa (solution left there)
+cudaError_t run_solve_c128(dct_plan* P, cplx* xa, int k, cudaStream_t st);
 cudaError_t launch_perm_in_any(const void* b, int b_dtype, int64_t bstride,
                                const int32_t* perm, int n, int k, int nbatch,
                                void* dst, int dst_dtype, cudaStream_t st);

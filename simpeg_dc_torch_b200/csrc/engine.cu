@@ -123,6 +123,32 @@ __global__ void k_gather_contract(int nbatch, int64_t n, int64_t nnz, int k,
   }
 }
 
+// complex128: gv[b, e] = -sum_r Y[b, row_e, r] X[b, col_e, r] (no
+// conjugation: the caller conjugates where its convention asks)
+__global__ void k_gather_contract_c(int nbatch, int64_t n, int64_t nnz, int k,
+                                    const int32_t* __restrict__ row,
+                                    const int32_t* __restrict__ col,
+                                    const cplx* __restrict__ Y, const cplx* __restrict__ X,
+                                    cplx* __restrict__ gv) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int64_t total = nnz * nbatch;
+  for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t < total;
+       t += warps) {
+    const int b = static_cast<int>(t / nnz);
+    const int64_t e = t - int64_t(b) * nnz;
+    const cplx* y = Y + (int64_t(b) * n + row[e]) * k;
+    const cplx* x = X + (int64_t(b) * n + col[e]) * k;
+    cplx acc;
+    for (int j = lane; j < k; j += 32) acc += y[j] * x[j];
+    for (int o = 16; o > 0; o >>= 1) {
+      acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+      acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+    }
+    if (lane == 0) gv[t] = -acc;
+  }
+}
+
 int report(cudaError_t e) {
   if (e == cudaSuccess) return DCT_OK;
   set_last_error(cudaGetErrorString(e));
@@ -210,7 +236,11 @@ int dct_gather_contract_plain(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
   if (nnz == 0) return DCT_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned g = blocks_for(nnz * nbatch * 32, kT);
-  if (dtype == DCT_F64)
+  if (dtype == DCT_C128)
+    k_gather_contract_c<<<g, kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, static_cast<const cplx*>(d_Y),
+        static_cast<const cplx*>(d_X), static_cast<cplx*>(d_gv));
+  else if (dtype == DCT_F64)
     k_gather_contract<double, false><<<g, kT, 0, st>>>(
         nbatch, n, nnz, k, d_row, d_col, nullptr, nullptr,
         static_cast<const double*>(d_Y), static_cast<const double*>(d_X),

@@ -31,9 +31,18 @@ namespace {
 
 template <typename T>
 __device__ __forceinline__ T load_val(const void* p, int dtype, int64_t i) {
+  if constexpr (sizeof(T) == sizeof(cplx)) {
+    if (dtype == DCT_C128) return static_cast<const cplx*>(p)[i];
+  }
   return dtype == DCT_F64 ? T(static_cast<const double*>(p)[i])
                           : T(static_cast<const float*>(p)[i]);
 }
+
+// resident CTAs per SM the trailing-update kernel is compiled for: two for
+// real values, one for complex (its 4 x 4 accumulators and tile copies are
+// twice as wide)
+template <typename T>
+constexpr int kUpdMinBlocks = sizeof(T) > 8 ? 1 : 2;
 
 // ---------------------------------------------------------------- small
 template <typename T>
@@ -296,7 +305,7 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 constexpr int kUT = kUpdateTile;
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kUpdMinBlocks<T>)
 k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
                int64_t front_stride, T* dinv, const int64_t* dinv_off,
                int64_t dinv_stride, int* status) {
@@ -548,7 +557,7 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
   T* fronts = static_cast<T*>(P->fronts);
   const int nb = P->nbatch;
   cudaError_t e = cudaSuccess;
-  const int small_max = sizeof(T) == 8 ? kSmallFrontF64 : kSmallFrontF32;
+  const int small_max = P->tune.small_front_max;
   const size_t small_smem = sizeof(T) * (size_t(small_max) * small_max + small_max);
   const size_t panel_smem = sizeof(T) * (2 * kPanel * kPanel);
   // the update kernel's tiles, or factor_diag's D and X, whichever is larger
@@ -648,6 +657,8 @@ cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,
                        int64_t vals_stride, cudaStream_t st) {
   if (P->dtype == DCT_F64)
     return factor_impl<double>(P, vals, vals_dtype, vals_stride, st);
+  if (P->dtype == DCT_C128)
+    return factor_impl<cplx>(P, vals, vals_dtype, vals_stride, st);
   return factor_impl<float>(P, vals, vals_dtype, vals_stride, st);
 }
 

@@ -46,7 +46,7 @@ __device__ __forceinline__ bool ir_skip(const int* skip) {
 // their shared memory admits 4 (float) / 2 (double); 3 caps float at 85
 // registers
 template <typename T>
-constexpr int kSolveMinBlocks = sizeof(T) == 4 ? 3 : 2;
+constexpr int kSolveMinBlocks = sizeof(T) == 4 ? 3 : (sizeof(T) == 8 ? 2 : 1);
 
 // S1 (the "a" operand) uses a padded leading dimension: several loaders
 // store it transposed, which would otherwise hit one bank 32 times.
@@ -704,6 +704,11 @@ cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st) {
   return solve_impl<double>(P, xa, static_cast<double*>(P->bufB), k, st);
 }
 
+// complex128 plans: as float64, on complex buffers
+cudaError_t run_solve_c128(dct_plan* P, cplx* xa, int k, cudaStream_t st) {
+  return solve_impl<cplx>(P, xa, static_cast<cplx*>(P->bufB), k, st);
+}
+
 // f32 plans: right-hand side in P->bufA (float, A), P->bufB (B).
 cudaError_t run_solve_f32(dct_plan* P, int k, cudaStream_t st) {
   return solve_impl<float>(P, static_cast<float*>(P->bufA),
@@ -714,6 +719,12 @@ cudaError_t launch_perm_in_any(const void* b, int b_dtype, int64_t bstride,
                                const int32_t* perm, int n, int k, int nbatch,
                                void* dst, int dst_dtype, cudaStream_t st) {
   dim3 g = grid1d(int64_t(n) * k, nbatch);
+  if (b_dtype == DCT_C128 || dst_dtype == DCT_C128) {
+    if (b_dtype != dst_dtype) return cudaErrorInvalidValue;
+    k_perm_in<cplx, cplx><<<g, kThreads, 0, st>>>(static_cast<const cplx*>(b), bstride, perm,
+                                                  n, k, static_cast<cplx*>(dst));
+    return cudaGetLastError();
+  }
   if (b_dtype == DCT_F64 && dst_dtype == DCT_F64)
     k_perm_in<double, double><<<g, kThreads, 0, st>>>(
         static_cast<const double*>(b), bstride, perm, n, k, static_cast<double*>(dst));
@@ -733,6 +744,12 @@ cudaError_t launch_perm_out_any(const void* src, int src_dtype, const int32_t* p
                                 int n, int k, int nbatch, void* x, int x_dtype,
                                 cudaStream_t st) {
   dim3 g = grid1d(int64_t(n) * k, nbatch);
+  if (src_dtype == DCT_C128 || x_dtype == DCT_C128) {
+    if (src_dtype != x_dtype) return cudaErrorInvalidValue;
+    k_perm_out<cplx, cplx><<<g, kThreads, 0, st>>>(static_cast<const cplx*>(src), perm, n, k,
+                                                   static_cast<cplx*>(x));
+    return cudaGetLastError();
+  }
   if (src_dtype == DCT_F64 && x_dtype == DCT_F64)
     k_perm_out<double, double><<<g, kThreads, 0, st>>>(
         static_cast<const double*>(src), perm, n, k, static_cast<double*>(x));

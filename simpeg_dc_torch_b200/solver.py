@@ -35,7 +35,9 @@ import torch
 
 from . import _native as nat
 
-_MATRIX_TYPES = ("spd",)
+# real SPD systems, and complex-symmetric ones (A^T = A, not Hermitian;
+# factored A = L L^T without conjugation)
+_MATRIX_TYPES = ("spd", "symmetric")
 
 
 def _require_cuda(device):
@@ -60,7 +62,15 @@ def _dtype_code(dt):
         return nat.F64
     if dt == torch.float32:
         return nat.F32
-    raise TypeError(f"unsupported dtype {dt}; float64 or float32 expected")
+    if dt in (torch.complex128, torch.complex64):
+        return nat.C128
+    raise TypeError(f"unsupported dtype {dt}; float64, float32 or complex expected")
+
+
+def _work_dtype(dt):
+    """The dtype of the buffers the library reads and writes: complex64
+    systems are factored and solved in complex128."""
+    return torch.complex128 if dt.is_complex else dt
 
 
 class _PlanSolver:
@@ -69,10 +79,12 @@ class _PlanSolver:
     def __init__(self, crow, col, n, n_rhs, nbatch, device, dtype,
                  matrix_type, coords, refine, leaf_size, refine_tol=None,
                  tuning=None):
-        if matrix_type not in _MATRIX_TYPES:
+        if matrix_type not in _MATRIX_TYPES or (
+                (matrix_type == "symmetric") != bool(dtype.is_complex)):
             raise NotImplementedError(
-                f"matrix_type {matrix_type!r}: only real SPD systems are "
-                "factored here (Cholesky)")
+                f"matrix_type {matrix_type!r} with dtype {dtype}: real SPD "
+                "systems ('spd', Cholesky) and complex-symmetric ones "
+                "('symmetric', L L^T) are factored here")
         self.device = _require_cuda(device)
         self.dtype = dtype
         self._code = _dtype_code(dtype)
@@ -135,7 +147,9 @@ class _PlanSolver:
     # ---- numeric phases
     def _factorize(self, values):
         v = values.detach()
-        if v.dtype not in (torch.float64, torch.float32):
+        if self._code == nat.C128:
+            v = v.to(torch.complex128)
+        elif v.dtype not in (torch.float64, torch.float32):
             v = v.to(torch.float64)
         v = v.to(self.device).contiguous()
         if v.dim() == 1:
@@ -153,11 +167,12 @@ class _PlanSolver:
         k = b2.shape[-1]
         if k > self.n_rhs:
             raise ValueError(f"{k} right-hand sides exceed n_rhs={self.n_rhs}")
-        x = torch.empty((self.nbatch, self.n, k), dtype=self.dtype,
-                        device=self.device)
-        self._plan.solve(b2.data_ptr(), self._code, 1 if batched else 0, k,
+        wdt = _work_dtype(self.dtype)
+        b2 = b2.to(wdt).contiguous()
+        x = torch.empty((self.nbatch, self.n, k), dtype=wdt, device=self.device)
+        self._plan.solve(b2.data_ptr(), _dtype_code(wdt), 1 if batched else 0, k,
                          x.data_ptr(), _stream_ptr(self.device))
-        return x
+        return x.to(self.dtype)
 
     def free(self):
         if getattr(self, "_plan", None) is not None:
@@ -214,11 +229,13 @@ def _grad_vals(solver, adj, x):
     """-sum_s adj[b, row_e, s] x[b, col_e, s] for every pattern entry."""
     nb = adj.shape[0]
     k = adj.shape[-1]
-    out = torch.empty((nb, solver.nnz), dtype=adj.dtype, device=adj.device)
+    wdt = _work_dtype(adj.dtype)
+    adj, x = adj.to(wdt).contiguous(), x.to(wdt).contiguous()
+    out = torch.empty((nb, solver.nnz), dtype=wdt, device=adj.device)
     nat.check(nat.lib().dct_gather_contract_plain(
         nb, solver.n, solver.nnz, k, solver.row.data_ptr(),
-        solver.col.data_ptr(), _dtype_code(adj.dtype),
-        adj.contiguous().data_ptr(), x.contiguous().data_ptr(),
+        solver.col.data_ptr(), _dtype_code(wdt),
+        adj.data_ptr(), x.data_ptr(),
         out.data_ptr(), _stream_ptr(solver.device)), "gather_contract")
     return out
 
@@ -239,14 +256,18 @@ class _SparseSolveFn(torch.autograd.Function):
     def backward(ctx, grad_x):
         (x,) = ctx.saved_tensors
         solver = ctx.solver
-        adj = solver.solve(grad_x.contiguous())
+        # complex-safe (a no-op on real tensors): torch hands backward the
+        # conjugate Wirtinger derivative G = dL/dx*; with A^T = A and x
+        # holomorphic in A, dL/dA*_ij = -conj(adj_i x_j), dL/db* = conj(adj)
+        # for adj = A^{-1} conj(G) (dctorch/solver.py:236-281)
+        adj = solver.solve(grad_x.conj().resolve_conj().contiguous())
         grad_vals = grad_b = None
         if ctx.needs_input_grad[0]:
             gv = _grad_vals(solver, adj.reshape(1, solver.n, -1),
                             x.reshape(1, solver.n, -1))
-            grad_vals = gv[0].to(ctx.dt_vals)
+            grad_vals = gv[0].conj().resolve_conj().to(ctx.dt_vals)
         if ctx.needs_input_grad[1]:
-            grad_b = adj.to(ctx.dt_b)
+            grad_b = adj.conj().resolve_conj().to(ctx.dt_b)
         return grad_vals, grad_b, None
 
 
@@ -272,13 +293,14 @@ class _SparseSolveBatchFn(torch.autograd.Function):
     def backward(ctx, grad_x):
         (x,) = ctx.saved_tensors
         solver = ctx.solver
-        adj = solver.solve(grad_x.contiguous())
+        # complex-safe, as _SparseSolveFn.backward
+        adj = solver.solve(grad_x.conj().resolve_conj().contiguous())
         grad_vals = grad_b = None
         if ctx.needs_input_grad[0]:
-            grad_vals = _grad_vals(solver, adj, x).to(ctx.dt_vals)
+            grad_vals = _grad_vals(solver, adj, x).conj().resolve_conj().to(ctx.dt_vals)
         if ctx.needs_input_grad[1]:
             gb = adj.sum(0) if ctx.b_shared else adj
-            grad_b = gb.to(ctx.dt_b)
+            grad_b = gb.conj().resolve_conj().to(ctx.dt_b)
         return grad_vals, grad_b, None
 
 

@@ -34,6 +34,11 @@ path in float64:
       tiny 2-D problem, background from the model and fixed: dpred, misfit,
       its gradient, Jtvec, chunked Jtvec and misfit_and_grad.  The primary
       is kept in host memory (no CUDA here: pin_memory is skipped).
+  cr_tiny.npz     : the complex-resistivity engine (dctorch/cr2d.py
+      TorchCR2D, complex-symmetric systems on SciPyBatchSolver's complex
+      SuperLU) on the tiny 2-D problem for both data conventions
+      ("magnitude", "real"): the (rho, ip) data of a stacked (log-rho,
+      chargeability) model and the gradient of its joint misfit.
   dcip_tiny.npz   : the joint non-linear DC + IP engine (dctorch/dcip2d.py
       TorchDCIP2D) on the tiny 2-D problem for both DC states: the DC and
       IP data of a stacked (log-rho, logit-eta) model and the gradient of
@@ -275,6 +280,7 @@ def main():
     np.savez_compressed(os.path.join(out, "ip_tiny.npz"),
                         **ip_fixture(a.reference, S, Q, S2, S3))
     np.savez_compressed(os.path.join(out, "dcip_tiny.npz"), **dcip_fixture(S, Q, S2))
+    np.savez_compressed(os.path.join(out, "cr_tiny.npz"), **cr_fixture(S, Q, S2))
     np.savez_compressed(os.path.join(out, "sr_tiny.npz"), **sr_fixture(Q, S2))
 
 
@@ -391,6 +397,43 @@ def dcip_fixture(S, Q, S2):
                     f"{state}_dobs_ip": dobs_ip, f"{state}_w_ip": w_ip,
                     f"{state}_phi": float(phi), f"{state}_grad": mt.grad.numpy()})
         print("dcip", state, "nD", d_dc.size, "max d_ip", float(np.abs(d_ip).max()))
+    return rec
+
+
+def cr_fixture(S, Q, S2):
+    import dctorch.cr2d as C2
+    mesh, survey, m = syn.tiny_2d()
+    ops = nodal_operators(mesh, survey)
+    rmin, rmax = electrode_distance_range(survey)
+    kys, wq, _ = Q.k0_quadrature(rmin, rmax, 7)
+    rec = dict(kys=kys, wq=wq, m_rho=m)
+    rng = np.random.default_rng(43)
+    chg = rng.uniform(0.01, 0.2, ops.nC)
+    for datum in ("magnitude", "real"):
+        eng, _ = engine_2d(S2, ops, kys, wq)
+        saved, S2.TorchDC2D = S2.TorchDC2D, (lambda *a, **k: eng)
+        try:
+            cr = C2.TorchCR2D(mesh, survey, nky=7, device="cpu",
+                              dtype=torch.complex128, ip_scale=1000.0,
+                              dc_datum=datum, quadrature=(kys, wq))
+        finally:
+            S2.TorchDC2D = saved
+        mm = np.concatenate([m, chg])
+        with torch.no_grad():
+            d_r, d_i = (x.numpy() for x in cr.dpred(torch.tensor(mm)))
+        dobs_r = d_r * (1.0 + 0.03 * rng.standard_normal(d_r.size))
+        w_r = 1.0 / (0.03 * np.abs(dobs_r) + 1e-3 * np.abs(dobs_r).max())
+        dobs_i = d_i + 2.0 * rng.standard_normal(d_i.size)
+        w_i = np.full(d_i.size, 0.5)
+        mt = torch.tensor(mm, requires_grad=True)
+        phi = cr.misfit(mt, torch.tensor(dobs_r), torch.tensor(w_r),
+                        torch.tensor(dobs_i), torch.tensor(w_i), lam=0.7)
+        phi.backward()
+        rec.update({f"{datum}_m": mm, f"{datum}_d_rho": d_r, f"{datum}_d_ip": d_i,
+                    f"{datum}_dobs_rho": dobs_r, f"{datum}_w_rho": w_r,
+                    f"{datum}_dobs_ip": dobs_i, f"{datum}_w_ip": w_i,
+                    f"{datum}_phi": float(phi), f"{datum}_grad": mt.grad.numpy()})
+        print("cr", datum, "nD", d_r.size, "max |d_ip|", float(np.abs(d_i).max()))
     return rec
 
 

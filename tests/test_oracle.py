@@ -148,6 +148,27 @@ def test_dcip_forward_matches_reference():
         assert O.rel(grad, J[f"{state}_grad"]) < 1e-9
 
 
+def test_cr_forward_matches_reference():
+    """The complex-resistivity forward and misfit gradient of the oracle
+    against the reference's TorchCR2D (dctorch/cr2d.py, complex SuperLU) on
+    the tiny 2-D problem, both data conventions."""
+    g = golden("dc2d_tiny")
+    op = _ops(g, False)
+    J = golden("cr_tiny")
+    assert np.array_equal(J["wq"], g["wq"])
+    n = J["m_rho"].size
+    for datum in ("magnitude", "real"):
+        mm = J[f"{datum}_m"]
+        d_rho, d_ip = O.cr_dpred_2d(op, mm[:n], mm[n:], 1000.0, datum)
+        assert O.rel(d_rho, J[f"{datum}_d_rho"]) < 1e-12
+        assert O.rel(d_ip, J[f"{datum}_d_ip"]) < 1e-10
+        phi, grad = O.cr_misfit_grad_2d(
+            op, mm, 1000.0, datum, J[f"{datum}_dobs_rho"], J[f"{datum}_w_rho"],
+            J[f"{datum}_dobs_ip"], J[f"{datum}_w_ip"], 0.7)
+        assert abs(phi - J[f"{datum}_phi"]) <= 1e-10 * abs(J[f"{datum}_phi"])
+        assert O.rel(grad, J[f"{datum}_grad"]) < 1e-9
+
+
 def test_singularity_removal_matches_reference():
     """The oracle's singularity-removed 2.5-D forward and gradient against
     the reference's TorchDC2D(singularity_removal=True) (golden sr_tiny);
