@@ -66,10 +66,10 @@ class FusedPath:
         plan = self.solver.plan
         self._plan = plan
         # float32 plans: most refinement corrections of the forward and of
-        # the adjoint fields (each stops early at the plan's tolerance).  One
-        # correction brings the data to ~1e-8, but the gradient contracts
-        # both fields at every node and needs two each (measured on the 3-D
-        # workload: 3e-3 with one, 3e-6 with two).
+        # the adjoint fields (each stops early at the plan's tolerance).  The
+        # gradient contracts both fields at every node, so their errors
+        # reach it amplified (measured on the 3-D benchmark: fields at
+        # 1e-10 give a gradient within 3e-6 of float64, at 5e-12 within 3e-9).
         self.refine_adj = self.solver.refine
         # with record_refinement set, every solve of the path synchronises
         # and keeps its refinement record in last_refinement (diagnostics)
