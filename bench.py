@@ -441,6 +441,7 @@ def main():
     ap.add_argument("--workload", default="dc3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -573,6 +574,20 @@ def main():
                                       + w_h.numel()) * 8,
                "d2h_bytes_per_step": (g_h.numel() + 1) * 8}
 
+    # the same eval+grad (misfit and gradient, no autograd) replayed from one
+    # CUDA graph of the whole launch sequence
+    graph = None
+    if not args.no_graph:
+        from simpeg_dc_torch_b200 import GraphedMisfitGrad
+        gmg = GraphedMisfitGrad(e32, m, dobs, w)
+        phi_g, g_g = gmg.replay(m)
+        graph_rel = float(torch.linalg.norm(g_g - g32) / torch.linalg.norm(g32))
+        graph_ms, _ = timed_loop(lambda: gmg.replay(m), args.steps, args.warmup)
+        graph = {"value": graph_ms, "unit": "ms", "launches": 1,
+                 "kernel_nodes": count_launches(e32),
+                 "grad_rel_vs_autograd": graph_rel}
+        del gmg
+
     # per-kernel-kind device time of one profiled eval+grad (CUDA events)
     plan = e32.solver.plan
     plan.profile(True, reset=True)
@@ -636,7 +651,7 @@ def main():
                         "parallelism": f"replicas x{world}"},
             "fp64_ms": ms64, "speedup_vs_fp64": ms64 / ms32,
             "accuracy_vs_fp64": acc, "refinement": refinement,
-            "e2e": e2e, "gpu_launches": count_launches(e32),
+            "e2e": e2e, "graph": graph, "gpu_launches": count_launches(e32),
             "roofline": roof,
             "kernel_ms": {k: v[0] / 2 for k, v in prof.items()},
             "cpu_baseline": cpu, "clocks": clocks,

@@ -9,7 +9,8 @@ reference's solver and engine interfaces:
     TorchDC2D, TorchDC3D, Linearization2D,
     TorchIP2D, TorchIP3D (linearized IP), TorchDCIP2D (joint DC + IP),
     TorchCR2D (complex resistivity, complex-symmetric systems),
-    TorchDC2DBatch (many uneven 2.5-D surveys in the same launches)
+    TorchDC2DBatch (many uneven 2.5-D surveys in the same launches),
+    GraphedMisfitGrad (an engine's eval + gradient replayed from a CUDA graph)
 
 Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
 discretize / SimPEG objects.  The engines also take a discretize
@@ -31,3 +32,4 @@ from .ip import TorchIP2D, TorchIP3D  # noqa: F401
 from .dcip import TorchDCIP2D  # noqa: F401
 from .cr2d import TorchCR2D  # noqa: F401
 from .batch import TorchDC2DBatch  # noqa: F401
+from .graphs import GraphedMisfitGrad  # noqa: F401

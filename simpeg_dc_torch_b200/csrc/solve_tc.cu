@@ -51,16 +51,27 @@ constexpr int kABytes = (kTcM / 8) * kASbo;                             // 9728
 constexpr uint32_t kBLbo = 128, kBSbo = (kStK / 4) * kBLbo + 16;       // 528
 constexpr int kBBytes = (kStN / 8) * kBSbo;                            // 16896
 constexpr int kSplitBytes = 2 * kABytes + 2 * kBBytes;
+// sets of split operands: with two, stage i is split into one set while the
+// MMAs of stage i - 1 still read the other
+#ifndef DCT_TC_SPLIT_SETS
+#define DCT_TC_SPLIT_SETS 1
+#endif
+constexpr int kSets = DCT_TC_SPLIT_SETS;
+static_assert(kSets == 1 || kSets == 2, "one or two split sets");
 // raw float32 stages as copied: A natural [k][m] with rows of kRawAld
 // floats, A transposed [m][k] with rows of kStK floats, B [k][n] with rows of
 // kRawBld floats (the padding keeps the converters' reads conflict-free)
-constexpr int kRaw = 2;
+#ifndef DCT_TC_RAW
+#define DCT_TC_RAW 2
+#endif
+constexpr int kRaw = DCT_TC_RAW;
+static_assert(kRaw >= 2 && kRaw <= 3, "two or three raw stages in flight");
 constexpr int kRawAld = kTcM + 8;
 constexpr int kRawABytes = kStK * kRawAld * 4;
 constexpr int kRawBld = kStN + 8;
 constexpr int kRawBBytes = kStK * kRawBld * 4;
 constexpr int kRawBytes = kRawABytes + kRawBBytes;
-constexpr size_t kSolveTcSmem = kSplitBytes + kRaw * size_t(kRawBytes) + 64;
+constexpr size_t kSolveTcSmem = kSets * size_t(kSplitBytes) + kRaw * size_t(kRawBytes) + 64;
 constexpr int kCtasPerSm = DCT_TC_CTAS_PER_SM;
 // output rows leave by bulk reductions (1) or float atomics (0)
 #ifndef DCT_TC_BULK_REDUCE
@@ -69,7 +80,7 @@ constexpr int kCtasPerSm = DCT_TC_CTAS_PER_SM;
 constexpr bool kTcBulkReduce = DCT_TC_BULK_REDUCE != 0;
 static_assert(kCtasPerSm * (kSolveTcSmem + 1024) <= 233472, "CTAs per SM");
 static_assert(kRawABytes >= kTcM * kStK * 4, "raw A holds both layouts");
-static_assert(64 * (kStN + 4) * 4 <= kSplitBytes + kRaw * kRawBytes,
+static_assert(64 * (kStN + 4) * 4 <= kSets * kSplitBytes + kRaw * kRawBytes,
               "64 staged output rows fit in the operand buffers");
 static_assert(kASbo % 16 == 0 && kABytes % 16 == 0 && kBSbo % 16 == 0 &&
                   kBBytes % 16 == 0 && kRawABytes % 16 == 0 && (kRawBld * 4) % 16 == 0,
@@ -101,8 +112,9 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   constexpr int kWarps = kNT / 32;
   static_assert(kWarps % 4 == 0, "whole warpgroups: TMEM lane quarters");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kSplitBytes + kRaw * kRawBytes);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  // one mbarrier per split set: the commits of the MMAs that read it
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + kSets * kSplitBytes + kRaw * kRawBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kSets);
   const PanelTask tk = g.tasks[blockIdx.x];
   const int b = blockIdx.y / g.nchunk;
   const int j0 = (blockIdx.y % g.nchunk) * kStN;
@@ -136,7 +148,8 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) tmem_alloc(tmem_slot, kStN);
-  if (tid == 0) mbar_init(&mbar[0]);
+  if (tid == 0)
+    for (int q = 0; q < kSets; ++q) mbar_init(&mbar[q]);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -144,16 +157,12 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
   const uint32_t idesc = umma_idesc_tf32(kTcM, np);
   const int nst = (k1 - k0 + kStK - 1) / kStK;
   bool ok = true;
-  unsigned char* Ahi = smem_raw;
-  unsigned char* Alo = Ahi + kABytes;
-  unsigned char* Bhi = Alo + kABytes;
-  unsigned char* Blo = Bhi + kBBytes;
   constexpr int kPerA = kTcM * kStK / kNT;          // 8 values
   constexpr int kPerB = kStN * kStK / 4 / kNT;      // 4 float4
   const bool vec4 = (g.k & 3) == 0;   // 16-byte aligned rows
   // stage st's float32 values -> raw slot st % kRaw (one commit group)
   auto issue_stage = [&](int st) {
-    unsigned char* raw = smem_raw + kSplitBytes + (st % kRaw) * kRawBytes;
+    unsigned char* raw = smem_raw + kSets * kSplitBytes + (st % kRaw) * kRawBytes;
     float* rA = reinterpret_cast<float*>(raw);
     float* rB = reinterpret_cast<float*>(raw + kRawABytes);
     const int kb = k0 + st * kStK;
@@ -231,23 +240,33 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
     kl = (c / kNc) * 4 + (lane & 3);
     n = ((c % kNc) * 8 + (lane >> 2)) * 4;
   };
-  if (nst > 0) issue_stage(0);
-  if (nst > 1) issue_stage(1);
+  for (int q = 0; q < kRaw && q < nst; ++q) issue_stage(q);
   for (int st = 0; st < nst; ++st) {
-    // this thread's copies of stage st have landed ...
-    if (st + 1 < nst)
+    // this thread's copies of stage st have landed (the groups of the
+    // stages after it may still be in flight) ...
+    const int pend = min(nst, st + kRaw) - st - 1;
+    if (pend >= 2)
+      asm volatile("cp.async.wait_group 2;" ::: "memory");
+    else if (pend == 1)
       asm volatile("cp.async.wait_group 1;" ::: "memory");
     else
       asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // ... and everyone's (the barrier), and the MMAs of stage st - 1, which
-    // read the split operands, have completed
-    if (st >= 1) {
-      ok = tc_wait(&mbar[0], uint32_t(st - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
+    // ... and everyone's (the barrier), and the MMAs of stage st - kSets,
+    // which read this stage's split set, have completed (the set's
+    // (st / kSets - 1)-th commit)
+    const int set = st % kSets;
+    if (st >= kSets) {
+      ok = tc_wait(&mbar[set], uint32_t(st / kSets - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT,
+                   s, b);
       if (!ok) break;
     } else {
       __syncthreads();
     }
-    const unsigned char* raw = smem_raw + kSplitBytes + (st % kRaw) * kRawBytes;
+    unsigned char* Ahi = smem_raw + set * kSplitBytes;
+    unsigned char* Alo = Ahi + kABytes;
+    unsigned char* Bhi = Alo + kABytes;
+    unsigned char* Blo = Bhi + kBBytes;
+    const unsigned char* raw = smem_raw + kSets * kSplitBytes + (st % kRaw) * kRawBytes;
     const float* rA = reinterpret_cast<const float*>(raw);
     const float* rB = reinterpret_cast<const float*>(raw + kRawABytes);
     const int kw = min(kStK, k1 - (k0 + st * kStK));
@@ -292,16 +311,17 @@ __global__ void __launch_bounds__(kNT, kCtasPerSm) k_solve_tc(SolveArgs<float> g
         umma_tf32(tmem, dah, dbl, idesc, 1u);
         umma_tf32(tmem, dal, dbh, idesc, 1u);
       }
-      umma_commit(&mbar[0]);
+      umma_commit(&mbar[set]);
     }
     // the next copies after the MMA issue: gathered rows wait on an index load
-    if (st + 2 < nst) issue_stage(st + 2);
+    if (st + kRaw < nst) issue_stage(st + kRaw);
   }
   // no copy may still be writing this CTA's shared memory when it exits
   asm volatile("cp.async.wait_all;" ::: "memory");
   // the last commit tracks every MMA issued before it
   if (ok && nst > 0)
-    ok = tc_wait(&mbar[0], uint32_t(nst - 1) & 1u, g.status, DCT_ERR_DEVICE_TIMEOUT, s, b);
+    ok = tc_wait(&mbar[(nst - 1) % kSets], uint32_t((nst - 1) / kSets) & 1u, g.status,
+                 DCT_ERR_DEVICE_TIMEOUT, s, b);
   const float sgn = kInv ? 1.0f : -1.0f;
   // rows 16-byte aligned and kc a multiple of 4: every output row of the
   // tile goes out as one bulk reduction (cp.reduce.async.bulk .add.f32) from
