@@ -605,10 +605,11 @@ def main():
         peaks = json.load(open(pk))
     hbm = peaks.get("hbm_gbs", 6650.0)
     tc = peaks.get("bf16_tflops", 1590.0)
-    traffic = None
+    traffic, traffic_launch = None, None
     tj = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tj):
-        traffic = json.load(open(tj)).get(args.workload, {}).get(dom)
+        tw = json.load(open(tj)).get(args.workload, {})
+        traffic, traffic_launch = tw.get(dom), tw.get(dom + "_launch")
     if dom in TENSOR_KINDS:
         ach = dfl / (dms * 1e-3) / 1e12
         roof = {"bound": "tensor", "achieved": ach, "peak": tc, "unit": "TFLOP/s",
@@ -626,7 +627,7 @@ def main():
                  "algorithmic_bytes_per_launch": dby / max(dn, 1),
                  "algorithmic_flops_per_launch": dfl / max(dn, 1),
                  "share_of_solver_time": dms / tot if tot else None,
-                 "traffic": traffic,
+                 "traffic": traffic, "traffic_launch": traffic_launch,
                  "peak_source": ("MEASURED_PEAKS.json (burst)" if peaks
                                  else "fallback")})
 
