@@ -332,6 +332,18 @@ int dct_solve_small_noalloc(int32_t n, const int32_t* d_crow,
                             const double* d_b, int32_t k, double* d_x,
                             void* stream);
 
+/* ---- self-test of the bounded device waits ---------------------------------
+ * No counterpart in the reference (failure detection).  Runs the kernels'
+ * bounded mbarrier wait on a barrier that nothing arrives on, with a limit of
+ * `polls` polls (1 .. 65536, each at most a few microseconds), on one CTA
+ * with no asynchronous operation in flight, and synchronises the stream.
+ * *code receives the status the wait recorded (DCT_ERR_DEVICE_TIMEOUT when
+ * it gave up, as a real stalled wait does in a plan's status words) and
+ * *completed (may be null) whether the wait saw its phase complete (0 here).
+ * The context stays usable afterwards. */
+int dct_selftest_wait_timeout(int32_t polls, int32_t* code, int32_t* completed,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

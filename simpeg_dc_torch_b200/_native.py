@@ -73,6 +73,7 @@ _SIGS = {
     "dct_symbolic_get_schedule": (C.c_int, [_p, _i32, _i32, _p, _pi64, _p,
                                             _pi64]),
     "dct_plan_create": (C.c_int, [_p, _i32, _i32, _i32, _i32, C.POINTER(_p)]),
+    "dct_selftest_wait_timeout": (C.c_int, [_i32, _pi32, _pi32, _p]),
     "dct_plan_create_tuned": (C.c_int, [_p, _i32, _i32, _i32, _i32,
                                         C.POINTER(Tuning), C.POINTER(_p)]),
     "dct_tuning_default": (C.c_int, [_i32, C.POINTER(Tuning)]),

@@ -119,14 +119,16 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parit
 
 // All threads: bounded wait for phase `parity` of the mbarrier; the result is
 // the same in every thread of the CTA.  Only warp 0 polls (the other warps
-// wait at the CTA barrier and issue nothing); at most kTcWaitLimit polls of
-// at most kTcSuspendNs each.  On timeout the first error is flagged.
+// wait at the CTA barrier and issue nothing); at most `limit` polls
+// (kTcWaitLimit unless given) of at most kTcSuspendNs each.  On timeout the
+// first error is flagged.
 __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity, int* status,
-                                        int code, int s, int b) {
+                                        int code, int s, int b,
+                                        uint32_t limit = kTcWaitLimit) {
   bool done = true;
   if (threadIdx.x < 32) {
     done = false;
-    for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it)
+    for (uint32_t it = 0; it < limit && !done; ++it)
       done = mbar_try_wait_sleep(smem_u32(bar), parity);
   }
   done = __syncthreads_and(done) != 0;
