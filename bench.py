@@ -442,6 +442,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--side", action="store_true",
+                    help="also time the complex-resistivity and DC-IP engines "
+                         "(2.5-D workloads)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -631,6 +634,37 @@ def main():
                  "peak_source": ("MEASURED_PEAKS.json (burst)" if peaks
                                  else "fallback")})
 
+    # the side engines on the same 2.5-D mesh and survey: complex resistivity
+    # (complex128 L L^T) and joint DC + IP (two float64 states), eval+grad
+    side = None
+    if args.side and args.workload in ("dc2d_small", "dc2d_large"):
+        from simpeg_dc_torch_b200 import TorchCR2D, TorchDCIP2D
+        nky = 12 if args.workload == "dc2d_large" else 11
+        chg = torch.tensor(np.random.default_rng(5).uniform(0.01, 0.2, m.numel()),
+                           device=dev)
+        side = {}
+        for name, eng, mm in (
+                ("cr2d_complex128", TorchCR2D(mesh, survey, nky=nky, device=dev,
+                                              ip_scale=1000.0), torch.cat([m, chg])),
+                ("dcip2d_float64", TorchDCIP2D(mesh, survey, nky=nky, device=dev,
+                                               eta_max=0.8, ip_scale=1000.0),
+                 torch.cat([m, torch.logit(chg / 0.8)]))):
+            with torch.no_grad():
+                d_a, d_b = eng.dpred(mm)
+            oa = d_a * 1.03
+            ob = d_b + 2.0
+            wa, wb = 1.0 / oa.abs(), torch.full_like(ob, 0.5)
+
+            def side_step(eng=eng, mm=mm, oa=oa, ob=ob, wa=wa, wb=wb):
+                x = mm.detach().requires_grad_(True)
+                eng.misfit(x, oa, wa, ob, wb, lam=0.7).backward()
+
+            ms_side, _ = timed_loop(side_step, args.steps, args.warmup)
+            eng.check()
+            side[name] = {"value": ms_side, "unit": "ms",
+                          "model": int(mm.numel()), "data": 2 * int(d_a.numel())}
+            del eng
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_leg(args.workload)
@@ -652,7 +686,8 @@ def main():
                         "parallelism": f"replicas x{world}"},
             "fp64_ms": ms64, "speedup_vs_fp64": ms64 / ms32,
             "accuracy_vs_fp64": acc, "refinement": refinement,
-            "e2e": e2e, "graph": graph, "gpu_launches": count_launches(e32),
+            "e2e": e2e, "graph": graph, "side_engines": side,
+            "gpu_launches": count_launches(e32),
             "roofline": roof,
             "kernel_ms": {k: v[0] / 2 for k, v in prof.items()},
             "cpu_baseline": cpu, "clocks": clocks,

@@ -40,14 +40,17 @@ class SuperLUBatch:
         self.lu = []
 
     def factorize(self, vals):
-        vals = np.atleast_2d(np.asarray(vals, float))
+        vals = np.atleast_2d(np.asarray(vals))
+        if not np.iscomplexobj(vals):
+            vals = vals.astype(float)
+        self.dtype = vals.dtype
         self.lu = [spla.splu(sp.csr_matrix((v, self.col, self.crow),
                                            shape=(self.n, self.n)).tocsc())
                    for v in vals]
 
     def solve(self, B):
         """B: (n, k) shared, or (nbatch, n, k); returns (nbatch, n, k)."""
-        B = np.asarray(B, float)
+        B = np.asarray(B, np.result_type(self.dtype, np.asarray(B).dtype, float))
         if B.ndim == 2:
             return np.stack([lu.solve(B) for lu in self.lu])
         return np.stack([lu.solve(B[i]) for i, lu in enumerate(self.lu)])
@@ -154,6 +157,80 @@ class SlabCholeskyBatch:
         """B: (n, k) shared, or (nbatch, n, k); returns (nbatch, n, k)."""
         B = np.asarray(B, float)
         with self._threads():
+            if B.ndim == 2:
+                return np.stack([self._solve_one(f, B) for f in self.fac])
+            return np.stack([self._solve_one(f, B[i]) for i, f in enumerate(self.fac)])
+
+
+class SlabLUBatch:
+    """Exact solves of nbatch systems on one grid pattern, real or complex
+    (complex-symmetric A of the complex-resistivity engine), by block
+    tridiagonal LU over the grid slabs (as `SlabCholeskyBatch`, without
+    symmetry): U_1 = A_11, L_i+1,i = A_i+1,i U_i^{-1},
+    U_i+1 = A_i+1,i+1 - L_i+1,i A_i,i+1, each U_i factored by dense LU with
+    partial pivoting inside the block (LAPACK getrf).  It computes the same
+    x = A^{-1} b as `SuperLUBatch` to rounding, which `tests/test_oracle.py`
+    checks."""
+
+    def __init__(self, crow, col, n, slab):
+        self._slab = SlabCholeskyBatch(crow, col, n, slab)
+        self.crow, self.col, self.n = self._slab.crow, self._slab.col, self._slab.n
+        self.order, self.starts = self._slab.order, self._slab.starts
+        self.fac = []
+
+    def factorize(self, vals):
+        import scipy.linalg as sla
+        vals = np.atleast_2d(np.asarray(vals))
+        if not np.iscomplexobj(vals):
+            vals = vals.astype(float)
+        self.dtype = vals.dtype
+        o, st = self.order, self.starts
+        self.fac = []
+        with self._slab._threads():
+            for v in vals:
+                A = sp.csr_matrix((v, self.col, self.crow), shape=(self.n, self.n))
+                A = A[o][:, o].tocsr()
+                lus, low, up = [], [], []
+                U = A[st[0]:st[1], st[0]:st[1]].toarray()
+                for i in range(len(st) - 1):
+                    a, b = st[i], st[i + 1]
+                    lu = sla.lu_factor(U, check_finite=False)
+                    lus.append(lu)
+                    if i + 2 < len(st):
+                        c = st[i + 2]
+                        Aup = A[a:b, b:c].toarray()
+                        Alo = A[b:c, a:b].toarray()
+                        # L = Alo U^{-1}:  U^T L^T = Alo^T
+                        Lb = _flush_tiny(sla.lu_solve(lu, Alo.T, trans=1,
+                                                      check_finite=False).T)
+                        low.append(Lb)
+                        up.append(Aup)
+                        U = A[b:c, b:c].toarray() - Lb @ Aup
+                self.fac.append((lus, low, up))
+
+    def _solve_one(self, f, B):
+        import scipy.linalg as sla
+        lus, low, up = f
+        st = self.starts
+        X = np.array(B[self.order], dtype=np.result_type(self.dtype, B.dtype))
+        ns = len(st) - 1
+        for i in range(1, ns):
+            a, b = st[i], st[i + 1]
+            X[a:b] -= low[i - 1] @ X[st[i - 1]:a]
+        for i in range(ns - 1, -1, -1):
+            a, b = st[i], st[i + 1]
+            rhs = X[a:b]
+            if i + 1 < ns:
+                rhs = rhs - up[i] @ X[b:st[i + 2]]
+            X[a:b] = _flush_tiny(sla.lu_solve(lus[i], rhs, check_finite=False))
+        out = np.empty_like(X)
+        out[self.order] = X
+        return out
+
+    def solve(self, B):
+        """B: (n, k) shared, or (nbatch, n, k); returns (nbatch, n, k)."""
+        B = np.asarray(B)
+        with self._slab._threads():
             if B.ndim == 2:
                 return np.stack([self._solve_one(f, B) for f in self.fac])
             return np.stack([self._solve_one(f, B[i]) for i, f in enumerate(self.fac)])
@@ -445,7 +522,8 @@ def cr_dpred_2d(op, m_rho, chg, ip_scale=1.0, dc_datum="magnitude",
     """Complex-resistivity 2.5-D data (dctorch/cr2d.py:74-97): the complex
     conductivity sigma* = sigma (1 - i m) with sigma = exp(-m_rho), complex
     values VALS = Lstack sigma*, U_k = A_k^{-1} q on complex SuperLU
-    (complex-symmetric A_k), Ubar = sum_k wq_k U_k, V = (Pd Ubar)[i, sidx_i];
+    (complex-symmetric A_k; the block LU `SlabLUBatch` when op carries grid
+    slabs), Ubar = sum_k wq_k U_k, V = (Pd Ubar)[i, sidx_i];
     d_rho = |V| ("magnitude") or Re V ("real"), d_ip = ip_scale Im V / Re V.
     Returns (d_rho, d_ip) or, with return_fields, also (V, sigma*, lu, U)."""
     nky = len(op["wq"])
@@ -454,10 +532,10 @@ def cr_dpred_2d(op, m_rho, chg, ip_scale=1.0, dc_datum="magnitude",
     L = op["Lstack"]
     VALS = (L @ sstar.real + 1j * (L @ sstar.imag)).reshape(nky, -1)
     n = op["nN"]
-    lu = [spla.splu(sp.csr_matrix((v, op["col"], op["crow"]), shape=(n, n)).tocsc())
-          for v in VALS]
-    Q = np.asarray(op["Q"], complex)
-    U = np.stack([f.solve(Q) for f in lu])
+    lu = (SlabLUBatch(op["crow"], op["col"], n, op["slab"]) if op.get("slab") is not None
+          else SuperLUBatch(op["crow"], op["col"], n))
+    lu.factorize(VALS)
+    U = lu.solve(np.asarray(op["Q"], complex))
     Ubar = np.tensordot(op["wq"], U, axes=(0, 0))
     PU = op["Pd"] @ Ubar
     V = PU[np.arange(PU.shape[0]), op["sidx"]]
@@ -502,9 +580,9 @@ def cr_misfit_grad_2d(op, m, ip_scale, dc_datum, dobs_rho, w_rho, dobs_ip, w_ip,
     r = row_of(op["crow"])
     nky = len(op["wq"])
     gv = np.empty((nky, len(op["col"])), complex)
+    Y = lu.solve(R)
     for k in range(nky):
-        Y = lu[k].solve(R)
-        gv[k] = -op["wq"][k] * np.einsum("es,es->e", Y[r], U[k][op["col"]])
+        gv[k] = -op["wq"][k] * np.einsum("es,es->e", Y[k][r], U[k][op["col"]])
     L = op["Lstack"]
     gvf = gv.reshape(-1)
     h = L.T @ gvf.real + 1j * (L.T @ gvf.imag)

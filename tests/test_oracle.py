@@ -169,6 +169,42 @@ def test_cr_forward_matches_reference():
         assert O.rel(grad, J[f"{datum}_grad"]) < 1e-9
 
 
+def test_slab_lu_matches_superlu_real_and_complex():
+    """The block-tridiagonal LU oracle solver against SuperLU on the tiny 2-D
+    pattern, with complex-symmetric values (sigma (1 - i m)) and real ones,
+    shared and per-system right-hand sides; and the complex-resistivity
+    oracle with it equals the one on SuperLU."""
+    from simpeg_dc_torch_b200 import synthetic as syn
+    g = golden("dc2d_tiny")
+    J = golden("cr_tiny")
+    op = _ops(g, False)
+    mesh, _, _ = syn.tiny_2d()
+    slab = O.grid_slabs(mesh.node_grid_index())
+    n = op["nN"]
+    rng = np.random.default_rng(12)
+    nC = op["Lstack"].shape[1]
+    sig = np.exp(rng.uniform(-3, 1, nC))
+    nnz = op["col"].size
+    for vals in (op["Lstack"][:2 * nnz] @ sig,
+                 op["Lstack"][:2 * nnz] @ sig - 1j * (op["Lstack"][:2 * nnz] @ (0.2 * sig))):
+        V = vals.reshape(2, nnz)
+        B = rng.standard_normal((n, 3)) + (1j * rng.standard_normal((n, 3))
+                                          if np.iscomplexobj(V) else 0)
+        a = O.SlabLUBatch(op["crow"], op["col"], n, slab)
+        a.factorize(V)
+        ref = O.SuperLUBatch(op["crow"], op["col"], n)
+        ref.factorize(V)
+        assert O.rel(a.solve(B), ref.solve(B)) < 1e-12
+        Bb = np.stack([B, 2 * B])
+        assert O.rel(a.solve(Bb), ref.solve(Bb)) < 1e-12
+    n2 = J["m_rho"].size
+    mm = J["magnitude_m"]
+    d0 = O.cr_dpred_2d(op, mm[:n2], mm[n2:], 1000.0)
+    op_s = dict(op, slab=slab)
+    d1 = O.cr_dpred_2d(op_s, mm[:n2], mm[n2:], 1000.0)
+    assert O.rel(d1[0], d0[0]) < 1e-12 and O.rel(d1[1], d0[1]) < 1e-11
+
+
 def test_singularity_removal_matches_reference():
     """The oracle's singularity-removed 2.5-D forward and gradient against
     the reference's TorchDC2D(singularity_removal=True) (golden sr_tiny);
