@@ -332,6 +332,26 @@ int dct_solve_small_noalloc(int32_t n, const int32_t* d_crow,
                             const double* d_b, int32_t k, double* d_x,
                             void* stream);
 
+/* ---- general (unsymmetric-valued) systems -----------------------------------
+ * Replaces cuDSS's "general" matrix type (dctorch/solver.py:44-47, the
+ * _MTYPE map: "general" -> GENERAL) for structurally symmetric patterns.
+ * A float64 plan that factors P A P^T = L U on the same symbolic analysis
+ * and schedules as the symmetric plans, without row exchanges: static
+ * pivoting replaces a pivot smaller than sqrt(eps) x the largest entry of its
+ * block (in magnitude) by that bound with the pivot's sign (counted, see
+ * dct_plan_static_pivots); a non-finite pivot records DCT_ERR_ZERO_PIVOT.
+ * Every pattern entry (i, j) needs its (j, i) (else DCT_ERR_BAD_PATTERN).
+ * dct_factorize takes float64 values of the whole pattern; dct_solve and
+ * dct_solve_permuted solve A x = b, dct_solve_transposed A^T x = b (the
+ * adjoint of a general solve) on the same factors. */
+int dct_plan_create_general(const dct_symbolic* sym, int32_t nbatch, int32_t max_rhs,
+                            int32_t device, dct_plan** out);
+int dct_solve_transposed(dct_plan* plan, const void* d_b, int32_t io_dtype,
+                         int32_t b_batched, int32_t k, void* d_x, void* stream);
+/* Number of pivots static pivoting replaced in the last factorization of a
+ * general plan (synchronises the stream). */
+int dct_plan_static_pivots(dct_plan* plan, void* stream, int32_t* count);
+
 /* ---- self-test of the bounded device waits ---------------------------------
  * No counterpart in the reference (failure detection).  Runs the kernels'
  * bounded mbarrier wait on a barrier that nothing arrives on, with a limit of

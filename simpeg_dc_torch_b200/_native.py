@@ -74,6 +74,9 @@ _SIGS = {
                                             _pi64]),
     "dct_plan_create": (C.c_int, [_p, _i32, _i32, _i32, _i32, C.POINTER(_p)]),
     "dct_selftest_wait_timeout": (C.c_int, [_i32, _pi32, _pi32, _p]),
+    "dct_plan_create_general": (C.c_int, [_p, _i32, _i32, _i32, C.POINTER(_p)]),
+    "dct_solve_transposed": (C.c_int, [_p, _p, _i32, _i32, _i32, _p, _p]),
+    "dct_plan_static_pivots": (C.c_int, [_p, _p, _pi32]),
     "dct_plan_create_tuned": (C.c_int, [_p, _i32, _i32, _i32, _i32,
                                         C.POINTER(Tuning), C.POINTER(_p)]),
     "dct_tuning_default": (C.c_int, [_i32, C.POINTER(Tuning)]),
@@ -215,16 +218,24 @@ class Symbolic:
 class Plan:
     """Numeric plan: nbatch systems on the pattern of `sym`, on one device."""
 
-    def __init__(self, sym: Symbolic, nbatch, max_rhs, dtype, device, tuning=None):
+    def __init__(self, sym: Symbolic, nbatch, max_rhs, dtype, device, tuning=None,
+                 general=False):
         h = _p()
         tu = None
         if tuning is not None:
             tu = Tuning(**{k: int(v) for k, v in dict(tuning).items()})
-        check(lib().dct_plan_create_tuned(sym.handle, int(nbatch), int(max_rhs),
-                                          int(dtype), int(device),
-                                          None if tu is None else C.byref(tu),
-                                          C.byref(h)),
-              "dct_plan_create_tuned")
+        if general:
+            # float64 L U with static pivoting (unsymmetric values)
+            check(lib().dct_plan_create_general(sym.handle, int(nbatch), int(max_rhs),
+                                                int(device), C.byref(h)),
+                  "dct_plan_create_general")
+        else:
+            check(lib().dct_plan_create_tuned(sym.handle, int(nbatch), int(max_rhs),
+                                              int(dtype), int(device),
+                                              None if tu is None else C.byref(tu),
+                                              C.byref(h)),
+                  "dct_plan_create_tuned")
+        self.general = bool(general)
         self._h = h
         self.sym = sym
         self.nbatch, self.max_rhs, self.dtype = int(nbatch), int(max_rhs), dtype
@@ -272,6 +283,16 @@ class Plan:
     def solve(self, d_b, io_dtype, b_batched, k, d_x, stream):
         check(lib().dct_solve(self._h, d_b, io_dtype, int(b_batched), int(k),
                               d_x, stream), "dct_solve")
+
+    def solve_transposed(self, d_b, io_dtype, b_batched, k, d_x, stream):
+        check(lib().dct_solve_transposed(self._h, d_b, io_dtype, int(b_batched), int(k),
+                                         d_x, stream), "dct_solve_transposed")
+
+    def static_pivots(self, stream):
+        n = C.c_int32(0)
+        check(lib().dct_plan_static_pivots(self._h, stream, C.byref(n)),
+              "dct_plan_static_pivots")
+        return n.value
 
     def solve_permuted(self, d_bp, b_batched, k, d_xp, stream):
         check(lib().dct_solve_permuted(self._h, d_bp, int(b_batched), int(k),

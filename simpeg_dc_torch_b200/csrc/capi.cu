@@ -892,6 +892,64 @@ int dct_plan_create_tuned(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs
   return DCT_OK;
 }
 
+int dct_plan_create_general(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs,
+                            int32_t device, dct_plan** out) {
+  if (!h || !out) return fail(DCT_ERR_ARG, "bad arguments");
+  *out = nullptr;
+  // the transpose map: entry (i, j) -> entry (j, i) of the input pattern,
+  // which must hold both (structurally symmetric)
+  const dct::Symbolic& S0 = h->sym;
+  const int n = S0.n;
+  std::vector<int32_t> tr(S0.in_col.size(), -1);
+  for (int i = 0; i < n; ++i)
+    for (int64_t e = S0.in_crow[i]; e < S0.in_crow[i + 1]; ++e) {
+      const int j = S0.in_col[e];
+      if (j < 0 || j >= n) return fail(DCT_ERR_BAD_PATTERN, "column out of range");
+      for (int64_t f = S0.in_crow[j]; f < S0.in_crow[j + 1]; ++f)
+        if (S0.in_col[f] == i) {
+          tr[e] = static_cast<int32_t>(f);
+          break;
+        }
+      if (tr[e] < 0)
+        return fail(DCT_ERR_BAD_PATTERN, "pattern not structurally symmetric: (i, j) without (j, i)");
+    }
+  dct_plan* P = nullptr;
+  int rc = dct_plan_create_tuned(h, nbatch, max_rhs, DCT_F64, device, nullptr, &P);
+  if (rc) return rc;
+  auto bail = [&](int code) {
+    dct_plan_destroy(P);
+    return code;
+  };
+  P->lu = 1;
+  // static pivoting at sqrt(eps) of the block's largest entry
+  P->pivot_floor = 1.4901161193847656e-08;
+  const int32_t* d_tr = nullptr;
+  if ((rc = upload(P, tr, &d_tr))) return bail(rc);
+  P->d_tr = d_tr;
+  if ((rc = alloc(P, 8 * size_t(P->sym.front_total) * nbatch, &P->fronts2, "front storage (U^T)")))
+    return bail(rc);
+  if ((rc = alloc(P, 8 * size_t(P->dinv_stride) * nbatch, &P->dinv2, "panel inverses (U^T)")))
+    return bail(rc);
+  if ((rc = alloc(P, 8 * size_t(P->linv_stride) * nbatch, &P->linv2,
+                  "supernode inverses (U^T)")))
+    return bail(rc);
+  *out = P;
+  return DCT_OK;
+}
+
+int dct_plan_static_pivots(dct_plan* P, void* stream, int32_t* count) {
+  if (!P || !count) return fail(DCT_ERR_ARG, "bad arguments");
+  int rc = set_device(P->device);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int h = 0;
+  DCT_CUDA(cudaMemcpyAsync(&h, P->status + 4, sizeof(int), cudaMemcpyDeviceToHost, st),
+           "status read");
+  DCT_CUDA(cudaStreamSynchronize(st), "stream synchronize");
+  *count = h;
+  return DCT_OK;
+}
+
 int dct_plan_set_refinement(dct_plan* P, int32_t iterations) {
   if (!P || iterations < 0 || iterations > 64) return fail(DCT_ERR_ARG, "bad arguments");
   P->ir_iters = iterations;
@@ -938,8 +996,13 @@ int dct_factorize(dct_plan* P, const void* d_vals, int32_t vals_dtype,
   if (!P || !d_vals || !valid_dtype(vals_dtype) ||
       ((vals_dtype == DCT_C128) != (P->dtype == DCT_C128)))
     return fail(DCT_ERR_ARG, "bad arguments (complex values need a complex plan and back)");
+  if (P->lu && vals_dtype != DCT_F64)
+    return fail(DCT_ERR_ARG, "general plans take float64 values");
   int rc = set_device(P->device);
   if (rc) return rc;
+  if (P->lu)
+    DCT_CUDA(cudaMemsetAsync(P->status + 4, 0, sizeof(int), static_cast<cudaStream_t>(stream)),
+             "static pivot count reset");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (P->dtype == DCT_F32) {
     // keep float64 values for the refinement residual
@@ -1010,8 +1073,25 @@ int dct_solve_permuted(dct_plan* P, const double* d_bp, int32_t b_batched,
   return solve_refined(P, d_bp, bstride, k, d_xp, st);
 }
 
+namespace {
+int solve_common(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
+                 int32_t k, void* d_x, void* stream, bool transposed);
+}  // namespace
+
 int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
               int32_t k, void* d_x, void* stream) {
+  return solve_common(P, d_b, io_dtype, b_batched, k, d_x, stream, false);
+}
+
+int dct_solve_transposed(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
+                         int32_t k, void* d_x, void* stream) {
+  if (P && !P->lu) return dct_solve(P, d_b, io_dtype, b_batched, k, d_x, stream);
+  return solve_common(P, d_b, io_dtype, b_batched, k, d_x, stream, true);
+}
+
+namespace {
+int solve_common(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
+                 int32_t k, void* d_x, void* stream, bool transposed) {
   if (!P || !d_b || !d_x || k < 1 || k > P->max_rhs || !valid_dtype(io_dtype) ||
       ((io_dtype == DCT_C128) != (P->dtype == DCT_C128)))
     return fail(DCT_ERR_ARG, "bad arguments");
@@ -1037,7 +1117,7 @@ int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
     DCT_CUDA(dct::launch_perm_in_any(d_b, io_dtype, bstride, P->ds.perm, n, k,
                                      P->nbatch, P->bufA, DCT_F64, st),
              "permute rhs");
-    DCT_CUDA(dct::run_solve_f64(P, static_cast<double*>(P->bufA), k, st),
+    DCT_CUDA(dct::run_solve_f64(P, static_cast<double*>(P->bufA), k, st, transposed),
              "solve launch");
     DCT_CUDA(dct::launch_perm_out_any(P->bufA, DCT_F64, P->ds.perm, n, k,
                                       P->nbatch, d_x, io_dtype, st),
@@ -1054,6 +1134,7 @@ int dct_solve(dct_plan* P, const void* d_b, int32_t io_dtype, int32_t b_batched,
            "permute solution");
   return DCT_OK;
 }
+}  // namespace
 
 int dct_plan_profile(dct_plan* P, int32_t enable, int32_t reset) {
   if (!P) return fail(DCT_ERR_ARG, "null plan");

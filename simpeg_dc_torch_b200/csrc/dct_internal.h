@@ -252,6 +252,17 @@ struct dct_plan {
   dct::IrState* ir = nullptr;      // device: refinement state of the last solve
   int update_bpan = 1;             // panels per trailing-update block
   dct::Profiler prof;
+  // general (unsymmetric-valued) float64 plans, factored P A P^T = L U with
+  // static pivoting: `fronts` holds L (unit diagonal) in the lower part,
+  // `fronts2` holds U^T in the lower part, both with the same layout; the
+  // inverses of L's diagonal blocks go to dinv / linv, those of U^T's to
+  // dinv2 / linv2.  d_tr maps every pattern entry (i, j) to the entry (j, i).
+  int lu = 0;
+  void* fronts2 = nullptr;
+  void* dinv2 = nullptr;
+  void* linv2 = nullptr;
+  const int32_t* d_tr = nullptr;
+  double pivot_floor = 0.0;        // relative static-pivot threshold (x max|block|)
 };
 
 struct dct_symbolic {
@@ -290,7 +301,8 @@ cudaError_t launch_update_tc(dct_plan* P, const PanelTask* tasks, int64_t count,
 void set_last_error(const char* msg);
 cudaError_t run_factor(dct_plan* P, const void* vals, int vals_dtype,
                        int64_t vals_stride, cudaStream_t st);
-cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st);
+cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st,
+                          bool transposed = false);
 cudaError_t run_solve_f32(dct_plan* P, int k, cudaStream_t st);
 // complex128 plans: the permuted right-hand side in xa (solution left there)
 cudaError_t run_solve_c128(dct_plan* P, cplx* xa, int k, cudaStream_t st);

@@ -23,6 +23,7 @@
 
 #include "dct_internal.h"
 #include "factor_diag.cuh"
+#include "factor_lu.cuh"
 #include "tile_mm.cuh"
 #include "tc_common.cuh"
 
@@ -144,18 +145,25 @@ k_small_front(DevSym S, const PanelTask* __restrict__ tasks, const void* vals,
 }
 
 // ------------------------------------------------------------ large: setup
+// general plans (fronts2 non-null): the transposed entries, through the
+// transpose map tr, go to the same positions of fronts2 (U^T's buffer)
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_large_scatter(DevSym S, const PanelTask* __restrict__ tasks, const void* vals,
                 int vals_dtype, int64_t vals_stride, T* fronts,
-                int64_t front_stride) {
+                int64_t front_stride, T* fronts2, const int32_t* __restrict__ tr) {
   const int s = tasks[blockIdx.x].s;
   const int b = blockIdx.y;
   T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  T* F2 = fronts2 == nullptr ? nullptr : fronts2 + int64_t(b) * front_stride + S.front_off[s];
   const int64_t a0 = S.amap_ptr[s], a1 = S.amap_ptr[s + 1];
-  for (int64_t q = a0 + threadIdx.x; q < a1; q += blockDim.x)
+  for (int64_t q = a0 + threadIdx.x; q < a1; q += blockDim.x) {
     F[S.amap_pos[q]] = load_val<T>(vals, vals_dtype,
                                    int64_t(b) * vals_stride + S.amap_e[q]);
+    if (F2 != nullptr)
+      F2[S.amap_pos[q]] = load_val<T>(vals, vals_dtype,
+                                      int64_t(b) * vals_stride + tr[S.amap_e[q]]);
+  }
 }
 
 // Zero the lower triangle (diagonal included) of the large fronts of a
@@ -304,39 +312,19 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 // t0 = -1: factor the diagonal block of panel p itself (a front's first panel).
 constexpr int kUT = kUpdateTile;
 
+// One tile update F_out[i, j] -= Fa_i Fb_j^T (K = w): rows ri.. of Fa and
+// rj.. of Fb in the panel's columns, 4 x 4 outputs per thread.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, kUpdMinBlocks<T>)
-k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
-               int64_t front_stride, T* dinv, const int64_t* dinv_off,
-               int64_t dinv_stride, int* status) {
-  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
-  pdl_trigger();
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* As = reinterpret_cast<T*>(smem_raw);   // [k][row of tile i], ld 64
-  T* Bs = As + kPanel * kUT;                // [k][row of tile j], ld 64
-  const PanelTask tk = tasks[blockIdx.x];
-  const int b = blockIdx.y;
-  const int s = tk.s;
-  const int N = S.front_n[s];
-  const int ns = S.sn_first[s + 1] - S.sn_first[s];
-  const int c0 = tk.p * kPanel;
-  const int w = min(kPanel, ns - c0);
-  const int base = c0 + w;
-  T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
-  T* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
+__device__ __forceinline__ void tile_update(const T* Fa, const T* Fb, T* Fo, int N, int c0,
+                                            int w, int ri, int rj, int ni, int nj, T* As,
+                                            T* Bs) {
   const int tid = threadIdx.x;
-  if (tk.t0 < 0) {
-    factor_diag<T, kThreads>(F, N, c0, w, As, Dv + int64_t(tk.p) * kPanel * kPanel, status, s, b);
-    return;
-  }
-  const int ri = base + tk.t0 * kUT, rj = base + tk.t1 * kUT;
-  const int ni = min(kUT, N - ri), nj = min(kUT, N - rj);
 #pragma unroll
   for (int idx = tid; idx < kPanel * kUT; idx += kThreads) {
     const int r = idx % kUT, k = idx / kUT;
     const bool kin = k < w;
-    As[idx] = (kin && r < ni) ? F[(ri + r) + int64_t(c0 + k) * N] : T(0);
-    Bs[idx] = (kin && r < nj) ? F[(rj + r) + int64_t(c0 + k) * N] : T(0);
+    As[idx] = (kin && r < ni) ? Fa[(ri + r) + int64_t(c0 + k) * N] : T(0);
+    Bs[idx] = (kin && r < nj) ? Fb[(rj + r) + int64_t(c0 + k) * N] : T(0);
   }
   __syncthreads();
   T acc[4][4];
@@ -352,19 +340,80 @@ k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int cc = ag + 16 * p, rr = jg + 16 * q;
-      cur[p][q] = (cc < nj && rr < ni) ? F[(ri + rr) + int64_t(rj + cc) * N] : T(0);
+      cur[p][q] = (cc < nj && rr < ni) ? Fo[(ri + rr) + int64_t(rj + cc) * N] : T(0);
     }
 #pragma unroll
   for (int p = 0; p < 4; ++p)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int cc = ag + 16 * p, rr = jg + 16 * q;
-      if (cc < nj && rr < ni) F[(ri + rr) + int64_t(rj + cc) * N] = cur[p][q] - acc[p][q];
+      if (cc < nj && rr < ni) Fo[(ri + rr) + int64_t(rj + cc) * N] = cur[p][q] - acc[p][q];
     }
+}
+
+// General plans (fronts2 non-null, float64): two products per tile, the lower
+// part of the trailing block in F1 -= L_i U_j^T-rows and its upper part,
+// transposed in F2, -= U^T_i L_j^T; diagonal blocks by lu_diag.
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kUpdMinBlocks<T>)
+k_large_update(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
+               int64_t front_stride, T* dinv, const int64_t* dinv_off,
+               int64_t dinv_stride, int* status, T* fronts2, T* dinv2, double pivot_floor) {
+  pdl_wait();   // launched with launch_pdl: the predecessor's writes first
+  pdl_trigger();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);   // [k][row of tile i], ld 64
+  T* Bs = As + kPanel * kUT;                // [k][row of tile j], ld 64
+  const PanelTask tk = tasks[blockIdx.x];
+  const int b = blockIdx.y;
+  const int s = tk.s;
+  const int N = S.front_n[s];
+  const int ns = S.sn_first[s + 1] - S.sn_first[s];
+  const int c0 = tk.p * kPanel;
+  const int w = min(kPanel, ns - c0);
+  const int base = c0 + w;
+  T* F = fronts + int64_t(b) * front_stride + S.front_off[s];
+  T* Dv = dinv + int64_t(b) * dinv_stride + dinv_off[s];
+  T* F2 = nullptr;
+  T* Dv2 = nullptr;
+  if constexpr (sizeof(T) == 8) {
+    if (fronts2 != nullptr) {
+      F2 = fronts2 + int64_t(b) * front_stride + S.front_off[s];
+      Dv2 = dinv2 + int64_t(b) * dinv_stride + dinv_off[s];
+    }
+  }
+  // the diagonal block of panel q (Cholesky and inverse, or LU and both
+  // inverses)
+  auto diag = [&](int q) {
+    const int cq = q * kPanel, wq = min(kPanel, ns - cq);
+    if constexpr (sizeof(T) == 8) {
+      if (F2 != nullptr) {
+        lu_diag<kThreads>(reinterpret_cast<double*>(F), reinterpret_cast<double*>(F2), N, cq,
+                          wq, reinterpret_cast<double*>(As),
+                          reinterpret_cast<double*>(Dv + int64_t(q) * kPanel * kPanel),
+                          reinterpret_cast<double*>(Dv2 + int64_t(q) * kPanel * kPanel),
+                          status, s, b, pivot_floor);
+        return;
+      }
+    }
+    factor_diag<T, kThreads>(F, N, cq, wq, As, Dv + int64_t(q) * kPanel * kPanel, status, s, b);
+  };
+  if (tk.t0 < 0) {
+    diag(tk.p);
+    return;
+  }
+  const int ri = base + tk.t0 * kUT, rj = base + tk.t1 * kUT;
+  const int ni = min(kUT, N - ri), nj = min(kUT, N - rj);
+  if (F2 == nullptr) {
+    tile_update<T>(F, F, F, N, c0, w, ri, rj, ni, nj, As, Bs);
+  } else {
+    tile_update<T>(F, F2, F, N, c0, w, ri, rj, ni, nj, As, Bs);
+    __syncthreads();   // the operand tiles are reloaded
+    tile_update<T>(F2, F, F2, N, c0, w, ri, rj, ni, nj, As, Bs);
+  }
   if (tk.t0 == 0 && tk.t1 == 0 && base < ns) {
     __syncthreads();   // this CTA's updates of the block are complete
-    factor_diag<T, kThreads>(F, N, base, min(kPanel, ns - base), As,
-                Dv + int64_t(tk.p + 1) * kPanel * kPanel, status, s, b);
+    diag(tk.p + 1);
   }
 }
 
@@ -516,7 +565,8 @@ k_linv_x(LinvArgs g, const T* ltmp, T* linv) {
 }
 
 template <typename T>
-cudaError_t run_linv(dct_plan* P, cudaStream_t st) {
+cudaError_t run_linv(dct_plan* P, cudaStream_t st, const void* fronts, const void* dinv,
+                     void* linv) {
   const int nb = P->nbatch;
   const size_t smem = sizeof(T) * ((kPanel + 1) * kPanel + kPanel * kPanel);
   cudaError_t e = cudaFuncSetAttribute(k_linv_t<T>,
@@ -536,15 +586,15 @@ cudaError_t run_linv(dct_plan* P, cudaStream_t st) {
     g.h = L.arg;
     dim3 grid(static_cast<unsigned>(L.count), nb);
     if (L.kind == kLinvInit)
-      k_linv_init<T><<<grid, kThreads, 0, st>>>(g, static_cast<const T*>(P->dinv),
-                                               static_cast<T*>(P->linv));
+      k_linv_init<T><<<grid, kThreads, 0, st>>>(g, static_cast<const T*>(dinv),
+                                               static_cast<T*>(linv));
     else if (L.kind == kLinvT)
-      k_linv_t<T><<<grid, kThreads, smem, st>>>(g, static_cast<const T*>(P->fronts),
-                                               static_cast<const T*>(P->linv),
+      k_linv_t<T><<<grid, kThreads, smem, st>>>(g, static_cast<const T*>(fronts),
+                                               static_cast<const T*>(linv),
                                                static_cast<T*>(P->ltmp));
     else
       k_linv_x<T><<<grid, kThreads, smem, st>>>(g, static_cast<const T*>(P->ltmp),
-                                               static_cast<T*>(P->linv));
+                                               static_cast<T*>(linv));
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = P->prof.end(st)) != cudaSuccess) return e;
   }
@@ -555,6 +605,9 @@ template <typename T>
 cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                         int64_t vals_stride, cudaStream_t st) {
   T* fronts = static_cast<T*>(P->fronts);
+  // general plans (float64 only): U^T's buffer
+  const bool lu = sizeof(T) == 8 && P->lu != 0;
+  T* fronts2 = lu ? static_cast<T*>(P->fronts2) : nullptr;
   const int nb = P->nbatch;
   cudaError_t e = cudaSuccess;
   const int small_max = P->tune.small_front_max;
@@ -568,6 +621,11 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
   e = cudaFuncSetAttribute(k_small_front<T>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(small_smem));
+  if constexpr (sizeof(T) == 8) {
+    if (e == cudaSuccess && lu)
+      e = cudaFuncSetAttribute(k_small_front_lu, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(small_smem));
+  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_large_panel<T>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -589,25 +647,46 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
     switch (L.kind) {
       case kSmallFront: {
         const size_t smem = sizeof(T) * (size_t(L.arg) * L.arg + L.arg);
+        if constexpr (sizeof(T) == 8) {
+          if (lu) {
+            k_small_front_lu<<<grid, kThreads, smem, st>>>(
+                P->ds, t, static_cast<const double*>(vals), vals_stride, P->d_tr,
+                reinterpret_cast<double*>(fronts), reinterpret_cast<double*>(fronts2),
+                P->front_stride, P->status, P->pivot_floor);
+            break;
+          }
+        }
         k_small_front<T><<<grid, kThreads, smem, st>>>(
             P->ds, t, vals, vals_dtype, vals_stride, fronts, P->front_stride,
             P->status);
         break;
       }
       case kLargeScatter:
-        k_zero_lower<T><<<dim3(static_cast<unsigned>(L.count), nb * kZeroSplit), kThreads,
-                          0, st>>>(P->ds, t, fronts, P->front_stride);
+        for (T* buf : {fronts, fronts2}) {
+          if (buf == nullptr) continue;
+          k_zero_lower<T><<<dim3(static_cast<unsigned>(L.count), nb * kZeroSplit), kThreads,
+                            0, st>>>(P->ds, t, buf, P->front_stride);
+        }
         k_large_scatter<T><<<grid, kThreads, 0, st>>>(
-            P->ds, t, vals, vals_dtype, vals_stride, fronts, P->front_stride);
+            P->ds, t, vals, vals_dtype, vals_stride, fronts, P->front_stride, fronts2,
+            P->d_tr);
         break;
       case kLargeExtendAdd:
-        k_large_extend_add<T><<<grid, kThreads, 0, st>>>(P->ds, t, fronts,
-                                                         P->front_stride);
+        for (T* buf : {fronts, fronts2}) {
+          if (buf == nullptr) continue;
+          k_large_extend_add<T><<<grid, kThreads, 0, st>>>(P->ds, t, buf, P->front_stride);
+        }
         break;
       case kLargePanel:
+        // general plans: L's rows take (U^T)^{-1} (L21 = A21 U11^{-1}), U^T's
+        // rows take L^{-1} (U12^T = A12^T L11^{-T})
         e = launch_pdl(k_large_panel<T>, grid, dim3(kThreads), panel_smem, st, P->ds, t, fronts,
-                       P->front_stride, static_cast<const T*>(P->dinv), P->d_dinv_off,
-                       P->dinv_stride, sizeof(T) == 4 ? P->img : ImgArgs{});
+                       P->front_stride, static_cast<const T*>(lu ? P->dinv2 : P->dinv),
+                       P->d_dinv_off, P->dinv_stride, sizeof(T) == 4 ? P->img : ImgArgs{});
+        if (e == cudaSuccess && lu)
+          e = launch_pdl(k_large_panel<T>, grid, dim3(kThreads), panel_smem, st, P->ds, t,
+                         fronts2, P->front_stride, static_cast<const T*>(P->dinv),
+                         P->d_dinv_off, P->dinv_stride, ImgArgs{});
         if (e != cudaSuccess) return e;
         break;
       case kLargeUpdate:
@@ -616,7 +695,8 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
         } else {
           e = launch_pdl(k_large_update<T>, grid, dim3(kThreads), update_smem, st, P->ds, t,
                          fronts, P->front_stride, static_cast<T*>(P->dinv), P->d_dinv_off,
-                         P->dinv_stride, P->status);
+                         P->dinv_stride, P->status, fronts2, static_cast<T*>(P->dinv2),
+                         P->pivot_floor);
         }
         if (e != cudaSuccess) return e;
         break;
@@ -643,12 +723,19 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
                          st>>>(P->ds, P->inv.d_tasks, fronts, P->front_stride,
                                static_cast<T*>(P->dinv), P->d_dinv_off,
                                P->dinv_stride);
+    if (lu)
+      k_panel_inverse<T><<<dim3(static_cast<unsigned>(ninv), nb), kThreads, inv_smem,
+                           st>>>(P->ds, P->inv.d_tasks, fronts2, P->front_stride,
+                                 static_cast<T*>(P->dinv2), P->d_dinv_off,
+                                 P->dinv_stride);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = P->prof.end(st);
     if (e != cudaSuccess) return e;
   }
-  return run_linv<T>(P, st);
+  e = run_linv<T>(P, st, P->fronts, P->dinv, P->linv);
+  if (e == cudaSuccess && lu) e = run_linv<T>(P, st, P->fronts2, P->dinv2, P->linv2);
+  return e;
 }
 
 }  // namespace

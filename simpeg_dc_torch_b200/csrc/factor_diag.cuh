@@ -108,7 +108,7 @@ __device__ __noinline__ void diag_leaf16(T* D, T* X, int o, int* status, int s, 
 
 template <typename T, int NT, bool FACTOR>
 __device__ __forceinline__ void diag_chol_inv(T* D, T* X, int* status, int s, int b) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   for (int kb = 0; kb < 4; ++kb) {
     const int o = kb * 16;
     if (warp == 0) diag_leaf16<T, FACTOR>(D, X, o, status, s, b);   // (a)

@@ -634,8 +634,11 @@ inline dim3 grid1d(int64_t total, int ny) {
   return dim3(static_cast<unsigned>(blocks), ny);
 }
 
+// transposed: solve A^T x = b (general plans: A^T = (L U)^T = M L^T with
+// M = U^T, so the forward pass runs on M and the backward pass on L)
 template <typename T>
-cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
+cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st,
+                       bool transposed = false) {
   const int nchunk = (k + kRC - 1) / kRC;
   const size_t smem3 = sizeof(T) * (kLD1 * kLD + 2 * kLD * kLD);
   cudaError_t e = cudaSuccess;
@@ -658,7 +661,22 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
   constexpr bool kTc = sizeof(T) == 4;
   const size_t work = sizeof(T) * size_t(P->nbatch) * P->sym.n * k;
   const double nb = P->nbatch;
+  // general plans: the forward pass runs on L (or M when transposed), the
+  // backward pass on the other factor, each with its own inverses
+  const T* fac[2] = {static_cast<const T*>(P->fronts), static_cast<const T*>(P->fronts)};
+  const T* dv[2] = {static_cast<const T*>(P->dinv), static_cast<const T*>(P->dinv)};
+  const T* lv[2] = {static_cast<const T*>(P->linv), static_cast<const T*>(P->linv)};
+  if (P->lu) {
+    const int m = transposed ? 0 : 1;   // the pass that runs on M = U^T
+    fac[m] = static_cast<const T*>(P->fronts2);
+    dv[m] = static_cast<const T*>(P->dinv2);
+    lv[m] = static_cast<const T*>(P->linv2);
+  }
   for (const Schedule* sc : {&P->fwd, &P->bwd}) {
+    const int pass = sc == &P->fwd ? 0 : 1;
+    g.fronts = fac[pass];
+    g.dinv = dv[pass];
+    g.linv = lv[pass];
     if (kTc) {
       e = cudaMemsetAsync(sc == &P->fwd ? static_cast<void*>(bufB) : static_cast<void*>(bufA),
                           0, work, st);
@@ -703,8 +721,9 @@ cudaError_t solve_impl(dct_plan* P, T* bufA, T* bufB, int k, cudaStream_t st) {
 
 // f64 plans: the permuted right-hand side is in `xa` (buffer A) and the
 // solution is left there; P->bufB serves as buffer B.
-cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st) {
-  return solve_impl<double>(P, xa, static_cast<double*>(P->bufB), k, st);
+cudaError_t run_solve_f64(dct_plan* P, double* xa, int k, cudaStream_t st,
+                          bool transposed) {
+  return solve_impl<double>(P, xa, static_cast<double*>(P->bufB), k, st, transposed);
 }
 
 // complex128 plans: as float64, on complex buffers

@@ -35,9 +35,10 @@ import torch
 
 from . import _native as nat
 
-# real SPD systems, and complex-symmetric ones (A^T = A, not Hermitian;
-# factored A = L L^T without conjugation)
-_MATRIX_TYPES = ("spd", "symmetric")
+# real SPD systems, complex-symmetric ones (A^T = A, not Hermitian;
+# factored A = L L^T without conjugation) and general real ones (float64
+# P A P^T = L U with static pivoting, structurally symmetric patterns)
+_MATRIX_TYPES = ("spd", "symmetric", "general")
 
 
 def _require_cuda(device):
@@ -80,11 +81,15 @@ class _PlanSolver:
                  matrix_type, coords, refine, leaf_size, refine_tol=None,
                  tuning=None):
         if matrix_type not in _MATRIX_TYPES or (
-                (matrix_type == "symmetric") != bool(dtype.is_complex)):
+                (matrix_type == "symmetric") != bool(dtype.is_complex)) or (
+                matrix_type == "general" and dtype != torch.float64):
             raise NotImplementedError(
                 f"matrix_type {matrix_type!r} with dtype {dtype}: real SPD "
-                "systems ('spd', Cholesky) and complex-symmetric ones "
-                "('symmetric', L L^T) are factored here")
+                "systems ('spd', Cholesky), complex-symmetric ones "
+                "('symmetric', L L^T) and float64 general ones ('general', "
+                "L U with static pivoting) are factored here")
+        self.matrix_type = matrix_type
+        self.general = matrix_type == "general"
         self.device = _require_cuda(device)
         self.dtype = dtype
         self._code = _dtype_code(dtype)
@@ -103,7 +108,8 @@ class _PlanSolver:
         self._sym = nat.Symbolic(crow_np, col_np, coords, leaf_size)
         with torch.cuda.device(self.device):
             self._plan = nat.Plan(self._sym, self.nbatch, self.n_rhs,
-                                  self._code, self.device.index, tuning)
+                                  self._code, self.device.index, tuning,
+                                  general=self.general)
         # refinement of float32 plans: at most `refine` corrections (the
         # library default is 2), fewer once the estimated error is below
         # `refine_tol` (0, the library default: a fixed count)
@@ -162,17 +168,24 @@ class _PlanSolver:
         self._vals_keepalive = v
         self.stamp += 1
 
-    def _solve(self, b2, batched):
-        """b2: (n, k) or (nbatch, n, k) in self.dtype; returns (nbatch, n, k)."""
+    def _solve(self, b2, batched, transposed=False):
+        """b2: (n, k) or (nbatch, n, k) in self.dtype; returns (nbatch, n, k).
+        transposed: solve A^T x = b (differs from A x = b for general plans)."""
         k = b2.shape[-1]
         if k > self.n_rhs:
             raise ValueError(f"{k} right-hand sides exceed n_rhs={self.n_rhs}")
         wdt = _work_dtype(self.dtype)
         b2 = b2.to(wdt).contiguous()
         x = torch.empty((self.nbatch, self.n, k), dtype=wdt, device=self.device)
-        self._plan.solve(b2.data_ptr(), _dtype_code(wdt), 1 if batched else 0, k,
-                         x.data_ptr(), _stream_ptr(self.device))
+        fn = self._plan.solve_transposed if transposed else self._plan.solve
+        fn(b2.data_ptr(), _dtype_code(wdt), 1 if batched else 0, k,
+           x.data_ptr(), _stream_ptr(self.device))
         return x.to(self.dtype)
+
+    def static_pivots(self):
+        """Pivots replaced by static pivoting in the last factorization of a
+        general plan (synchronises the stream); 0 for the other types."""
+        return self._plan.static_pivots(_stream_ptr(self.device)) if self.general else 0
 
     def free(self):
         if getattr(self, "_plan", None) is not None:
@@ -194,11 +207,12 @@ class DCTSolver(_PlanSolver):
         """Numeric refactorization with new values (nnz,), same pattern."""
         self._factorize(values.reshape(1, -1))
 
-    def solve(self, b):
-        """Solve A x = b for the current factorization; b (n,) or (n, k)."""
+    def solve(self, b, transposed=False):
+        """Solve A x = b (A^T x = b with transposed) for the current
+        factorization; b (n,) or (n, k)."""
         b2 = b.detach().to(device=self.device, dtype=self.dtype)
         b2 = b2.reshape(self.n, -1).contiguous()
-        x = self._solve(b2, False)
+        x = self._solve(b2, False, transposed)
         return x[0].reshape(b.shape)
 
 
@@ -217,11 +231,12 @@ class DCTBatchSolver(_PlanSolver):
         """values: (nbatch, nnz) -- refactorize every system."""
         self._factorize(values)
 
-    def solve(self, b):
-        """b: (nbatch, n, k) or shared (n, k); returns (nbatch, n, k)."""
+    def solve(self, b, transposed=False):
+        """b: (nbatch, n, k) or shared (n, k); returns (nbatch, n, k)
+        (A^T x = b with transposed)."""
         shared = b.dim() == 2
         b2 = b.detach().to(device=self.device, dtype=self.dtype).contiguous()
-        return self._solve(b2, not shared)
+        return self._solve(b2, not shared, transposed)
 
 
 # --------------------------------------------------------------- autograd
@@ -257,10 +272,12 @@ class _SparseSolveFn(torch.autograd.Function):
         (x,) = ctx.saved_tensors
         solver = ctx.solver
         # complex-safe (a no-op on real tensors): torch hands backward the
-        # conjugate Wirtinger derivative G = dL/dx*; with A^T = A and x
-        # holomorphic in A, dL/dA*_ij = -conj(adj_i x_j), dL/db* = conj(adj)
-        # for adj = A^{-1} conj(G) (dctorch/solver.py:236-281)
-        adj = solver.solve(grad_x.conj().resolve_conj().contiguous())
+        # conjugate Wirtinger derivative G = dL/dx*; with x holomorphic in A,
+        # dL/dA*_ij = -conj(adj_i x_j), dL/db* = conj(adj) for
+        # adj = A^{-T} conj(G) (dctorch/solver.py:236-281, where A^T = A); a
+        # general plan solves with A^T on the same factors
+        adj = solver.solve(grad_x.conj().resolve_conj().contiguous(),
+                           transposed=getattr(solver, "general", False))
         grad_vals = grad_b = None
         if ctx.needs_input_grad[0]:
             gv = _grad_vals(solver, adj.reshape(1, solver.n, -1),
@@ -293,8 +310,9 @@ class _SparseSolveBatchFn(torch.autograd.Function):
     def backward(ctx, grad_x):
         (x,) = ctx.saved_tensors
         solver = ctx.solver
-        # complex-safe, as _SparseSolveFn.backward
-        adj = solver.solve(grad_x.conj().resolve_conj().contiguous())
+        # complex-safe, as _SparseSolveFn.backward (A^T for general plans)
+        adj = solver.solve(grad_x.conj().resolve_conj().contiguous(),
+                           transposed=getattr(solver, "general", False))
         grad_vals = grad_b = None
         if ctx.needs_input_grad[0]:
             grad_vals = _grad_vals(solver, adj, x).conj().resolve_conj().to(ctx.dt_vals)
