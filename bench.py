@@ -65,6 +65,13 @@ WORKLOADS = {
                        l2="inputs larger than L2 (float32 fronts of 64 surveys)",
                        flush=False),
     # a reduced 3-D case for profiler captures (a few GB on the device)
+    "dc3d_tree": dict(desc="3-D DC, octree TreeMesh (2:1 balanced, 5 m finest cells "
+                           "refined around a 21x21 surface grid at 10 m, 293,868 "
+                           "cells, 286,960 free nodes), 400 gradient-array sources "
+                           "x 40 dipoles (16,000 data), Gaussian random field "
+                           "log-rho (50 m correlation, sigma 0.5)",
+                      l2="inputs larger than L2 (fields 0.92 GB in float64)",
+                      flush=False),
     "dc3d_mid": dict(desc="3-D DC, TensorMesh 40x40x20 core @8 m + 6 padding/face "
                           "(x1.3), same 200 sources and 6,000 data",
                      l2="inputs larger than L2 (float32 fronts 0.62 GB)",
@@ -85,6 +92,15 @@ REFERENCE_3D_UNAVAILABLE = (
     "node system measured at 951.6 s, solves at 23.8 s per 10 right-hand sides, "
     "200 sources forward + 200 adjoint), so warm-up + timed steps cannot finish "
     "in a bench run; no smaller grid stands in for it")
+REFERENCE_TREE_UNAVAILABLE = (
+    "the reference builds TreeMesh operators through SimPEG/discretize, which "
+    "are absent, and its CPU path (float64 SuperLU, single-threaded) on this "
+    "286,960-node octree system with 400 sources (factor + 800 right-hand "
+    "sides) exceeds the ~1,900 s measured for the 269,001-node tensor case")
+
+
+def _unavailable_reason(name):
+    return REFERENCE_TREE_UNAVAILABLE if name == "dc3d_tree" else REFERENCE_3D_UNAVAILABLE
 
 
 def build_case(name, seed):
@@ -93,6 +109,8 @@ def build_case(name, seed):
         return syn.dc3d(seed=seed)
     if name == "dc3d_mid":
         return syn.dc3d(seed=seed, ncore=(40, 40, 20), dx=8.0, npad=6)
+    if name == "dc3d_tree":
+        return syn.dc3d_tree(seed=seed)
     if name == "dc2d_large":
         return syn.dc2d_large(seed=seed)
     if name == "dc2d_batch":
@@ -116,7 +134,7 @@ def make_engine(name, mesh, survey, device, dtype):
         import torch
         return TorchDC2DBatch(mesh, nky=12, device=device, dtype=dtype,
                               tune=dtype == torch.float32)
-    if name in ("dc3d", "dc3d_mid"):
+    if name in ("dc3d", "dc3d_mid", "dc3d_tree"):
         return TorchDC3D(mesh, survey, device=device, dtype=dtype)
     nky = 12 if name == "dc2d_large" else 11
     return TorchDC2D(mesh, survey, nky=nky, device=device, dtype=dtype)
@@ -350,7 +368,7 @@ def run_reference(args):
     if args.workload.startswith("dc3d"):
         print(json.dumps({"impl": "reference", "metric": METRIC,
                           "config": workload_config(args.workload),
-                          "unavailable": REFERENCE_3D_UNAVAILABLE}), flush=True)
+                          "unavailable": _unavailable_reason(args.workload)}), flush=True)
         return 0
     ref = ReferenceCpu(args.workload)
     for _ in range(args.warmup):
@@ -415,7 +433,7 @@ def cpu_baseline_leg(name):
     the 3-D workloads, the reason it cannot run with the full-size record."""
     if name.startswith("dc3d"):
         out = {"value": None, "unit": "ms", "cores": 1, "kind": "port",
-               "sample": "none", "unavailable": REFERENCE_3D_UNAVAILABLE}
+               "sample": "none", "unavailable": _unavailable_reason(name)}
         if name == "dc3d":
             # 951.6 s factorization + 2 x 200 right-hand sides at 2.38 s each
             out["recorded_full_size_estimate_ms"] = 1e3 * (951.6 + 2 * 200 * 2.38)

@@ -48,7 +48,7 @@ class FusedPath:
 
     def __init__(self, crow, col, L, w, Q, Pd, sidx, device, precision,
                  coords=None, refine=None, n_rhs=None, refine_fields=None,
-                 refine_tol=None, tuning=None, leaf_size=64):
+                 refine_tol=None, tuning=None, leaf_size=64, refine_tol_fields=None):
         self.device = device
         nN = crow.size - 1
         self.nN, self.nnzA = nN, col.size
@@ -77,6 +77,10 @@ class FusedPath:
         self.last_refinement = {}
         self.refine_fields = (self.refine_adj if refine_fields is None
                               else int(refine_fields))
+        # stopping tolerances of the forward-field and of the adjoint
+        # solves (0: a fixed number of corrections)
+        self.tol_adj = self.solver.refine_tol
+        self.tol_fields = self.tol_adj if refine_tol_fields is None else float(refine_tol_fields)
         self._iperm_ptr = plan.d_iperm
         perm = self.solver._sym.array("perm")
         iperm = np.empty_like(perm)
@@ -164,13 +168,17 @@ class FusedPath:
                                   self._st())
         return x
 
+    def _set_refinement(self, iters, tol):
+        self._plan.set_refinement(iters)
+        self._plan.set_refinement_tolerance(tol)
+
     def _record(self, what):
         if self.record_refinement and self.solver.dtype == torch.float32:
             self.last_refinement[what] = self.solver.refinement_info()
 
     def fields(self):
         """U = A^{-1} Q, permuted (nbatch, nN, nS)."""
-        self._plan.set_refinement(self.refine_fields)
+        self._set_refinement(self.refine_fields, self.tol_fields)
         U = self._solve_perm(self._scatter(self._q, None, self.nS), self.nS)
         self._record("fields")
         return U
@@ -213,7 +221,7 @@ class FusedPath:
             rho = torch.exp(m_full.detach().to(self.device, torch.float64)[p["cell"]])
         Xs = (p["X"] * rho.view(1, 1, -1)).contiguous()
         rhs = p["R1"] + self._pattern_product(vals.reshape(-1).contiguous(), Xs, -1.0)
-        self._plan.set_refinement(self.refine_fields)
+        self._set_refinement(self.refine_fields, self.tol_fields)
         Us = torch.empty_like(rhs)
         self._plan.solve_permuted(rhs.data_ptr(), 1, self.nS, Us.data_ptr(), self._st())
         self._record("fields")
@@ -248,7 +256,7 @@ class FusedPath:
         """dL/dm_full for dL/dd = gd on the current factorization."""
         g = gd.detach().to(self.device, torch.float64).contiguous()
         R = self._scatter(self._adj, g, self.nS)
-        self._plan.set_refinement(self.refine_adj)
+        self._set_refinement(self.refine_adj, self.tol_adj)
         Y = self._solve_perm(R, self.nS)
         self._record("adjoint")
         gv = torch.empty(self.nbatch * self.nnzA, dtype=torch.float64,
@@ -285,7 +293,7 @@ class FusedPath:
             self.col_e.data_ptr(), self._iperm_ptr, dvals.data_ptr(),
             self.nnzA, -1.0, U.data_ptr(), rhs.data_ptr(), self._st()),
             "dct_pattern_spmm")
-        self._plan.set_refinement(self.refine_fields)
+        self._set_refinement(self.refine_fields, self.tol_fields)
         dU = torch.empty_like(rhs)
         self._plan.solve_permuted(rhs.data_ptr(), 1, k, dU.data_ptr(), self._st())
         return self.project(dU)
@@ -301,7 +309,7 @@ class FusedPath:
         rhs.index_put_((self.iperm_d[self.Pd_col[p0:p1].long()],
                         self.Pd_row[p0:p1] - a), self.Pd_val[p0:p1],
                        accumulate=True)
-        self._plan.set_refinement(self.refine_adj)
+        self._set_refinement(self.refine_adj, self.tol_adj)
         Y = self._solve_perm(rhs, nb)
         gv = torch.empty((self.nbatch * self.nnzA, nb), dtype=torch.float64,
                          device=self.device)

@@ -209,9 +209,13 @@ def as_tensor_mesh(mesh):
     any tensor mesh that exposes discretize's public `h` (per-axis widths)
     and `origin` (or `x0`), such as `discretize.TensorMesh`
     (dctorch/simulation2d.py:37-40 and simulation3d.py:47-48 take those).
-    Other mesh types (a discretize `TreeMesh`, ...) raise NotImplementedError."""
+    This package's `TreeMesh` passes through; other mesh types (a discretize
+    `TreeMesh`, ...) raise NotImplementedError."""
     if isinstance(mesh, TensorMesh):
         return mesh
+    from .treemesh import TreeMesh
+    if isinstance(mesh, TreeMesh):
+        return mesh          # this package's tree meshes pass through
     kind = str(getattr(mesh, "_meshType", "TENSOR")).upper()
     if kind != "TENSOR" or not hasattr(mesh, "h"):
         raise NotImplementedError(

@@ -80,6 +80,12 @@ class NodalOperators:
             alpha[nt] = (ky * k1e(kr) / k0e(kr) * rdn)[nt]
         coef = alpha * f["area"] / f["nodes"].shape[1]
         npf = f["nodes"].shape[1]
+        if "exp_pos" in f:
+            # tree meshes: each face's corner terms through the hanging-node
+            # interpolation (entries off the diagonal included)
+            fc = f["exp_face"]
+            return sp.csr_matrix((coef[fc] * f["exp_w"], (f["exp_pos"], f["cell"][fc])),
+                                 shape=(self.nnzA, self.nC))
         rows = np.repeat(f["diag_pos"], 1).reshape(-1)
         vals = np.repeat(coef, npf)
         cells = np.repeat(f["cell"], npf)
@@ -206,7 +212,11 @@ def _boundary_faces(mesh, pos_of):
 
 def nodal_operators(mesh, survey) -> NodalOperators:
     """Assemble the sigma-linear maps, sources and receivers for a tensor mesh
-    (this package's, or any with discretize's public `h` and `origin`)."""
+    (this package's, or any with discretize's public `h` and `origin`) or a
+    `TreeMesh` of this package."""
+    from .treemesh import TreeMesh
+    if isinstance(mesh, TreeMesh):
+        return tree_nodal_operators(mesh, survey)
     mesh = as_tensor_mesh(mesh)
     dim = mesh.dim
     nC, nN = mesh.nC, mesh.n_nodes
@@ -286,5 +296,154 @@ def nodal_operators(mesh, survey) -> NodalOperators:
     return NodalOperators(
         dim=dim, nC=nC, nN=nN, nnzA=nnzA,
         crow=indptr.astype(np.int32), col=indices.astype(np.int32),
+        L_edge=L_edge, L_node=L_node, bc_faces=bcf, q=q, Pd=Pd,
+        sidx=np.asarray(sidx, dtype=np.int64))
+
+
+# ------------------------------------------------------------------ trees
+def _outer_entries(G, weights):
+    """For every row r of the sparse G (rows x n): the entries
+    weights[r] * G[r, i] * G[r, j] of the rank-one term G[r]^T G[r], as
+    (i, j, value, r) arrays."""
+    G = sp.csr_matrix(G)
+    G.sum_duplicates()
+    nnz_row = np.diff(G.indptr)
+    I, J, V, R = [], [], [], []
+    for k in np.unique(nnz_row):
+        if k == 0:
+            continue
+        rows = np.flatnonzero(nnz_row == k)
+        starts = G.indptr[rows]
+        idx = starts[:, None] + np.arange(k)[None, :]
+        cols = G.indices[idx]
+        vals = G.data[idx]
+        cols = cols.astype(np.int64)          # i n + j keys exceed 32 bits
+        I.append(np.repeat(cols, k, axis=1).reshape(-1))
+        J.append(np.tile(cols, (1, k)).reshape(-1))
+        V.append((vals[:, :, None] * vals[:, None, :] * weights[rows][:, None, None]).reshape(-1))
+        R.append(np.repeat(rows, k * k))
+    if not I:
+        e = np.zeros(0, np.int64)
+        return e, e, np.zeros(0), e
+    return np.concatenate(I), np.concatenate(J), np.concatenate(V), np.concatenate(R)
+
+
+def tree_nodal_operators(mesh, survey) -> NodalOperators:
+    """The sigma-linear maps, sources and receivers on a `TreeMesh`: the
+    tensor-mesh operators cell by cell on all leaf corners, mapped to the
+    free nodes through the hanging-node interpolation P (see treemesh.py)."""
+    from .treemesh import TreeMesh
+    if not isinstance(mesh, TreeMesh) or not mesh._final:
+        raise ValueError("a finalized TreeMesh is expected")
+    dim = mesh.dim
+    nC, nN = mesh.nC, mesh.n_nodes
+    Pm = mesh.P.tocsr()
+    n_all = Pm.shape[0]
+    cn = mesh._cell_nodes                     # (nC, 2^dim) all-node ids, x fastest
+    size = mesh._cell_size
+    vol = mesh.cell_volumes
+    # ---- element edges: rows (cell, edge), G = (E1 - E0) P
+    e0, e1, wts, cells = [], [], [], []
+    for ax in range(dim):
+        ln = size * mesh.h0[ax]
+        for k in range(2 ** dim):
+            if (k >> ax) & 1:
+                continue
+            e0.append(cn[:, k])
+            e1.append(cn[:, k | (1 << ax)])
+            wts.append(vol / 2 ** (dim - 1) / ln ** 2)
+            cells.append(np.arange(nC))
+    e0, e1 = np.concatenate(e0), np.concatenate(e1)
+    wts, cells = np.concatenate(wts), np.concatenate(cells)
+    nr = e0.size
+    E = sp.csr_matrix((np.r_[np.ones(nr), -np.ones(nr)],
+                       (np.r_[np.arange(nr), np.arange(nr)], np.r_[e1, e0])),
+                      shape=(nr, n_all))
+    G = (E @ Pm).tocsr()
+    gi, gj, gv, gr = _outer_entries(G, wts)
+    # ---- nodal mass: rows (cell, corner), vector P[corner]
+    Mr = sp.csr_matrix((np.ones(nC * 2 ** dim), (np.arange(nC * 2 ** dim), cn.reshape(-1))),
+                       shape=(nC * 2 ** dim, n_all))
+    Nm = (Mr @ Pm).tocsr()
+    mw = np.repeat(vol / 2 ** dim, 2 ** dim)
+    mi, mj, mv, mr = _outer_entries(Nm, mw)
+    mcell = mr // (2 ** dim)
+    # ---- boundary faces (all but the top): geometry and corner vectors
+    nf = mesh.n_finest
+    lo = mesh._cell_lo
+    fcell, fctr, fnrm, farea, fnodes, ftop = [], [], [], [], [], []
+    for ax in range(dim):
+        others = [o for o in range(dim) if o != ax]
+        for side in (0, 1):
+            on = (lo[:, ax] == 0) if side == 0 else (lo[:, ax] + size == nf)
+            c = np.flatnonzero(on)
+            if c.size == 0:
+                continue
+            ctr = mesh.origin + (lo[c] + 0.5 * size[c, None]) * mesh.h0
+            ctr[:, ax] = mesh.origin[ax] + (0 if side == 0 else nf) * mesh.h0[ax]
+            nv = np.zeros((c.size, dim))
+            nv[:, ax] = -1.0 if side == 0 else 1.0
+            ar = np.ones(c.size)
+            for o in others:
+                ar = ar * size[c] * mesh.h0[o]
+            ks = [k for k in range(2 ** dim) if ((k >> ax) & 1) == side]
+            fcell.append(c)
+            fctr.append(ctr)
+            fnrm.append(nv)
+            farea.append(ar)
+            fnodes.append(cn[c][:, ks])
+            ftop.append(np.full(c.size, ax == dim - 1 and side == 1))
+    fcell = np.concatenate(fcell)
+    fctr, fnrm = np.vstack(fctr), np.vstack(fnrm)
+    farea, fnodes = np.concatenate(farea), np.vstack(fnodes)
+    ftop = np.concatenate(ftop)
+    npf = fnodes.shape[1]
+    Fr = sp.csr_matrix((np.ones(fnodes.size), (np.arange(fnodes.size), fnodes.reshape(-1))),
+                       shape=(fnodes.size, n_all))
+    Fm = (Fr @ Pm).tocsr()
+    bi, bj, bv, br = _outer_entries(Fm, np.ones(fnodes.size))
+    bface = br // npf
+    # ---- the A pattern: every entry any term touches, plus the diagonal
+    keys = np.unique(np.concatenate([gi * nN + gj, mi * nN + mj, bi * nN + bj,
+                                     np.arange(nN, dtype=np.int64) * (nN + 1)]))
+    rows_k, cols_k = keys // nN, keys % nN
+    indptr = np.zeros(nN + 1, np.int64)
+    np.add.at(indptr, rows_k + 1, 1)
+    indptr = np.cumsum(indptr)
+    nnzA = keys.size
+
+    def pos(i, j):
+        return np.searchsorted(keys, np.asarray(i, np.int64) * nN + np.asarray(j, np.int64))
+
+    L_edge = sp.csr_matrix((gv, (pos(gi, gj), cells[gr])), shape=(nnzA, nC))
+    L_edge.sum_duplicates()
+    L_edge.sort_indices()
+    L_node = sp.csr_matrix((mv, (pos(mi, mj), mcell)), shape=(nnzA, nC))
+    L_node.sum_duplicates()
+    L_node.sort_indices()
+    nodes_all = mesh.nodes
+    middle = np.median(nodes_all, axis=0)
+    src_pt = np.r_[middle[:-1], np.max(nodes_all[:, -1])]
+    rv = fctr - src_pt
+    r = np.linalg.norm(rv, axis=-1)
+    rdn = np.einsum("ij,ij->i", rv / r[:, None], fnrm)
+    bcf = {"r": r, "r_dot_n": rdn, "area": farea, "cell": fcell,
+           "nodes": fnodes, "not_top": ~ftop,
+           # the P-mapped corner terms: entry, face, weight
+           "exp_pos": pos(bi, bj), "exp_face": bface, "exp_w": bv}
+    qcols = [sp.csc_matrix(source_term(src, mesh).reshape(-1, 1))
+             for src in survey.source_list]
+    q = sp.hstack(qcols).tocsc() if qcols else sp.csc_matrix((nN, 0))
+    Pb, sidx = [], []
+    for isrc, src in enumerate(survey.source_list):
+        for rx in src.receiver_list:
+            P = receiver_projection(rx, mesh)
+            Pb.append(P)
+            sidx += [isrc] * P.shape[0]
+    Pd = sp.vstack(Pb).tocsr() if Pb else sp.csr_matrix((0, nN))
+    Pd.sort_indices()
+    return NodalOperators(
+        dim=dim, nC=nC, nN=nN, nnzA=nnzA,
+        crow=indptr.astype(np.int32), col=cols_k.astype(np.int32),
         L_edge=L_edge, L_node=L_node, bc_faces=bcf, q=q, Pd=Pd,
         sidx=np.asarray(sidx, dtype=np.int64))

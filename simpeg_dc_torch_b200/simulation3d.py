@@ -5,14 +5,18 @@ Same recipe as the 2.5-D engine without wavenumbers: one assembly map
 L3 = L_edge + L_bc (Robin), one system factored once per evaluation, all
 sources solved as right-hand sides of that factorization, and the adjoint
 reusing it.  `dtype=torch.float32` selects the float32 factor/solve with
-float64 iterative refinement; data and misfit are float64 either way.  Each
-refined solve takes at most `refine` corrections (default 2) and stops once
-the estimated relative error of its solution is below `refine_tol` (default
-1e-11).  Measured on the 269,001-node benchmark: the forward fields reach
-1e-10 after one correction and 5e-12 after two, the adjoint fields 2e-12
-after one, so the default runs two corrections forward and one adjoint; the
-misfit gradient then agrees with float64 (and with four corrections each) to
-3e-9.  A count with refine_tol=0 runs a fixed number of corrections.
+float64 iterative refinement; data and misfit are float64 either way.  The
+forward fields take `refine_fields` corrections (default 2, a fixed count);
+the adjoint solves at most `refine` (default 2), stopping once the estimated
+relative error of the adjoint fields is below `refine_tol` (default 1e-11).
+The gradient contracts both fields at every node, so the forward fields'
+error reaches it amplified by up to ~1e7 (the size of the misfit weights of
+near-zero data): measured on the 286,960-node octree workload, one forward
+correction (estimated error 4.6e-12) leaves the gradient 4.8e-5 off, two
+leave it 1e-8 off; the adjoint fields reach 1e-12 after one correction and a
+second changes the gradient by less than 1e-9 (on the 269,001-node tensor
+benchmark as well).  refine_tol_fields > 0 makes the forward count
+adaptive too.
 """
 from __future__ import annotations
 
@@ -32,7 +36,7 @@ class TorchDC3D:
     def __init__(self, mesh, survey, device="cuda", dtype=torch.float64,
                  active_cells=None, val_inactive=None, bc_type="Robin",
                  refine=None, refine_fields=None, refine_tol=None,
-                 leaf_size=64):
+                 leaf_size=64, refine_tol_fields=0.0):
         if bc_type != "Robin":
             raise NotImplementedError("only the Robin boundary condition is built")
         self.device = torch.device(device)
@@ -60,7 +64,8 @@ class TorchDC3D:
                                refine=refine, refine_fields=refine_fields,
                                leaf_size=leaf_size,
                                refine_tol=(1e-11 if refine_tol is None
-                                           else refine_tol))
+                                           else refine_tol),
+                               refine_tol_fields=refine_tol_fields)
         self.solver = self._path.solver
         self.sidx = torch.as_tensor(ops.sidx, device=self.device)
         self.iD = torch.arange(self.nD, device=self.device)

@@ -274,6 +274,79 @@ def dc3d(seed=0, ncore=(64, 64, 32), dx=5.0, npad=8, n_grid=10,
     return mesh, survey, m
 
 
+def gaussian_random_field(points, rng, corr=50.0, sigma=0.5, spacing=None, extent=None):
+    """A seeded smooth random field at `points` (n, dim): white noise on a
+    regular grid filtered by a Gaussian kernel of correlation length `corr`
+    (FFT), scaled to standard deviation `sigma`, interpolated linearly."""
+    from scipy.interpolate import RegularGridInterpolator
+    pts = np.atleast_2d(np.asarray(points, float))
+    lo = pts.min(0) if extent is None else np.asarray(extent[0], float)
+    hi = pts.max(0) if extent is None else np.asarray(extent[1], float)
+    d = corr / 4.0 if spacing is None else float(spacing)
+    n = [int(np.ceil((h - l) / d)) + 1 for l, h in zip(lo, hi)]
+    noise = rng.standard_normal(n)
+    k = np.meshgrid(*[np.fft.fftfreq(m, d=d) for m in n], indexing="ij")
+    k2 = sum(ki ** 2 for ki in k)
+    field = np.real(np.fft.ifftn(np.fft.fftn(noise) * np.exp(-0.5 * (2 * np.pi) ** 2 * k2 *
+                                                              (corr / 2.0) ** 2)))
+    field = (field - field.mean()) / (field.std() + 1e-30) * sigma
+    axes = [l + d * np.arange(m) for l, m in zip(lo, n)]
+    f = RegularGridInterpolator(axes, field, bounds_error=False, fill_value=None)
+    return f(np.clip(pts, lo, hi))
+
+
+def dc3d_tree(seed=0, max_level=8, h0=5.0, n_el=21, spacing=10.0, n_sources=400, n_rx=40,
+              refine=((8, 130.0), (7, 250.0), (6, 400.0), (5, 600.0))):
+    """Config 5: a 3-D octree refined around a surface electrode grid
+    (n_el x n_el at `spacing`), gradient-array sources (far-apart A, B pairs,
+    each with n_rx adjacent-electrode potential dipoles between them) and a
+    Gaussian random field log-rho (50 m correlation, sigma 0.5 around
+    log 100).  Returns (mesh, survey, m)."""
+    from .treemesh import TreeMesh
+    rng = np.random.default_rng(seed)
+    nf = 2 ** max_level
+    width = nf * h0
+    tm = TreeMesh([(h0, nf)] * 3, origin=[-width / 2, -width / 2, -width])
+    half = (n_el - 1) * spacing / 2
+    g = np.linspace(-half, half, n_el)
+    ex, ey = np.meshgrid(g, g, indexing="ij")
+    elec = np.c_[ex.ravel(), ey.ravel(), np.zeros(ex.size)]
+    tm.refine(lambda lo, hi: np.full(lo.shape[0], 3))
+    for level, pad in refine:
+        tm.refine_points(elec, level, padding=pad)
+    tm.finalize()
+    idx = np.arange(elec.shape[0]).reshape(n_el, n_el)
+    pairs = np.r_[np.c_[idx[:-1, :].ravel(), idx[1:, :].ravel()],
+                  np.c_[idx[:, :-1].ravel(), idx[:, 1:].ravel()]]
+    mid = 0.5 * (elec[pairs[:, 0]] + elec[pairs[:, 1]])
+    srcs = []
+    while len(srcs) < n_sources:
+        a, b = rng.choice(elec.shape[0], 2, replace=False)
+        A, B = elec[a], elec[b]
+        if np.linalg.norm(A - B) < 0.6 * (2 * half):
+            continue
+        # dipoles in the middle third between A and B (the gradient array's
+        # potential electrodes), nearest to the segment first
+        t = np.clip(((mid - A) @ (B - A)) / ((B - A) @ (B - A)), 0.0, 1.0)
+        dseg = np.linalg.norm(mid - (A + t[:, None] * (B - A)), axis=1)
+        ok = (t > 1 / 3) & (t < 2 / 3)
+        ok &= np.all(pairs != a, axis=1) & np.all(pairs != b, axis=1)
+        order = np.argsort(np.where(ok, dseg, np.inf))[:n_rx]
+        rx = DipoleReceiver(elec[pairs[order, 0]], elec[pairs[order, 1]])
+        srcs.append(DipoleSource([rx], A, B))
+    survey = Survey(srcs)
+    m = np.log(100.0) + gaussian_random_field(tm.cell_centers, rng, corr=50.0, sigma=0.5,
+                                              spacing=10.0,
+                                              extent=(tm.origin, tm.origin + width))
+    return tm, survey, m
+
+
+def tree_small(seed=0):
+    """A small 3-D octree case (a few thousand nodes) for parity tests."""
+    return dc3d_tree(seed=seed, max_level=6, h0=5.0, n_el=5, spacing=10.0, n_sources=6,
+                     n_rx=4, refine=((6, 8.0), (5, 20.0), (4, 45.0)))
+
+
 def observed(d_true, rng, rel_noise=0.05):
     """dobs = d (1 + rel N(0,1)), w = 1 / (rel |dobs|) (the workloads' noise)."""
     dobs = d_true * (1.0 + rel_noise * rng.standard_normal(d_true.shape))
