@@ -12,8 +12,9 @@ reference's solver and engine interfaces:
     TorchDC2DBatch (many uneven 2.5-D surveys in the same launches),
     GraphedMisfitGrad (an engine's eval + gradient replayed from a CUDA graph)
 
-Mesh/survey helpers (`TensorMesh`, `Survey`, sources, receivers) stand in for
-discretize / SimPEG objects.  The engines also take a discretize
+Mesh/survey helpers (`TensorMesh`, `TreeMesh` -- octree / quadtree with
+hanging nodes --, `Survey`, sources, receivers) stand in for discretize /
+SimPEG objects.  The engines also take a discretize
 `TensorMesh` (or any tensor mesh with its public `h` and `origin`) and
 SimPEG-shaped DC surveys (`source_list`, `location_a/b`, `locations_m/n`,
 `current`), reading only those public attributes.
@@ -21,6 +22,7 @@ SimPEG-shaped DC surveys (`source_list`, `location_a/b`, `locations_m/n`,
 __version__ = "0.1.0"
 
 from .mesh import TensorMesh  # noqa: F401
+from .treemesh import TreeMesh  # noqa: F401
 from .survey import (DipoleReceiver, DipoleSource, PoleReceiver,  # noqa: F401
                      PoleSource, Survey)
 from .solver import (CuDSSBatchSolver, CuDSSSolver, DCTBatchSolver,  # noqa: F401
