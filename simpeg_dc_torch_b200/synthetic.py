@@ -297,7 +297,7 @@ def gaussian_random_field(points, rng, corr=50.0, sigma=0.5, spacing=None, exten
 
 def dc3d_tree(seed=0, max_level=8, h0=5.0, n_el=21, spacing=10.0, n_sources=400, n_rx=40,
               refine=((8, 130.0), (7, 250.0), (6, 400.0), (5, 600.0))):
-    """Config 5: a 3-D octree refined around a surface electrode grid
+    """The refined 3-D workload: an octree refined around a surface electrode grid
     (n_el x n_el at `spacing`), gradient-array sources (far-apart A, B pairs,
     each with n_rx adjacent-electrode potential dipoles between them) and a
     Gaussian random field log-rho (50 m correlation, sigma 0.5 around

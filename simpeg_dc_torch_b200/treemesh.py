@@ -328,6 +328,10 @@ class TreeMesh:
             raise AssertionError("point outside every leaf")
         return self._cell_code_order[pos]
 
+    def point2index(self, locs):
+        """discretize's name: the cell containing each point."""
+        return self.cells_of_points(locs)
+
     def get_interpolation_matrix(self, locs, location_type="N"):
         """discretize's name: nodal ("N") interpolation onto the free nodes."""
         if location_type not in ("N", "nodes"):

@@ -1,8 +1,8 @@
 """Linearised products of the 2.5-D engine on the GPU: TorchDC2D.Jmatrix /
 Jvec and Linearization2D (Jvec, Jtvec, diag_JtDJ, Jmatrix) against the
 reference's own outputs (golden fixture dc2d_lin, made by running
-dctorch/simulation2d.py:439-818) and against the CPU oracle on the C1
-workload.  The reference's own spec for J is 1e-12 against its Jtvec
+dctorch/simulation2d.py:439-818) and against the CPU oracle on the small
+2.5-D workload.  The reference's own spec for J is 1e-12 against its Jtvec
 (dctorch/tests/test_jmatrix.py:77-79); float64 here is held to 1e-10,
 float32 + refinement to 1e-6."""
 import numpy as np

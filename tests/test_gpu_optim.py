@@ -51,7 +51,7 @@ def pcg(apply_H, b, Minv, maxiter, rtol):
 
 
 def test_lbfgs_iteration_on_the_3d_benchmark(cuda):
-    """Config 4 (269,001 nodes, 200 sources), float32 + refinement engine."""
+    """The 3-D benchmark (269,001 nodes, 200 sources), float32 + refinement engine."""
     mesh, survey, m_true = syn.dc3d(seed=0)
     e32 = TorchDC3D(mesh, survey, device=cuda, dtype=torch.float32)
     with torch.no_grad():
@@ -95,7 +95,7 @@ def test_lbfgs_iteration_on_the_3d_benchmark(cuda):
 
 
 def test_gauss_newton_step_on_the_2d_large_workload(cuda):
-    """Config 2 (56,525 nodes, 12 wavenumbers, 186 sources), float64."""
+    """The large 2.5-D workload (56,525 nodes, 12 wavenumbers, 186 sources), float64."""
     mesh, survey, m_true = syn.dc2d_large(seed=0)
     eng = TorchDC2D(mesh, survey, nky=12, device=cuda)
     with torch.no_grad():

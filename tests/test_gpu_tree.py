@@ -1,14 +1,14 @@
-"""The 3-D engine on an octree (the config-5 workload's mesh type, at a small
+"""The 3-D engine on an octree (the refined 3-D workload's mesh type, at a small
 size): float64 and float32 + refinement against the oracle (SuperLU on the
 tree operators), the float64 adjoint gradient against central finite
-differences on 20 random directions (config 5's check), and ten L-BFGS
+differences on 20 random directions (that workload's check), and ten L-BFGS
 iterations of the float32 engine (its optimizer contract)."""
 import numpy as np
 import pytest
 import torch
 
 from oracle import dc_oracle as O
-from simpeg_dc_torch_b200 import TorchDC3D
+from simpeg_dc_torch_b200 import TorchDC2D, TorchDC3D, TreeMesh
 from simpeg_dc_torch_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -99,3 +99,39 @@ def test_tree_lbfgs_ten_iterations(cuda):
     eng.check()
     assert len(values) >= 3
     assert min(values) < 0.5 * values[0]
+
+
+def test_quadtree_2p5d_engine_against_oracle(cuda):
+    """The 2.5-D engine on a quadtree refined along the electrode line
+    (hanging nodes in every wavenumber system), float64 and float32 +
+    refinement against the oracle."""
+    tm = TreeMesh([(1.0, 128)] * 2, origin=[-64.0, -128.0])
+    tm.refine(lambda lo, hi: np.full(lo.shape[0], 3))
+    xe = np.linspace(-20.0, 20.0, 11)
+    el = np.c_[xe, np.zeros_like(xe)]
+    for level, pad in ((7, 4.0), (6, 12.0), (5, 30.0)):
+        tm.refine_points(el, level, padding=pad)
+    tm.finalize()
+    assert tm.n_hanging_nodes > 0
+    mesh_survey = syn.dipole_dipole_2d(xe, 4, a=1)
+    from simpeg_dc_torch_b200.survey import Survey
+    survey = Survey(mesh_survey)
+    rng = np.random.default_rng(8)
+    m = np.log(100.0) + 0.3 * rng.standard_normal(tm.nC)
+    for dtype in (torch.float64, torch.float32):
+        eng = TorchDC2D(tm, survey, nky=8, device=cuda, dtype=dtype)
+        o = eng._ops
+        op = dict(Lstack=eng._L, crow=o.crow, col=o.col, nN=o.nN, Q=o.q.toarray(), Pd=o.Pd,
+                  sidx=o.sidx, wq=eng.wq_np)
+        d_ref = O.dpred_2d(op, m)
+        dobs, w = syn.observed(d_ref, np.random.default_rng(9))
+        phi_ref, g_ref = O.misfit_grad_2d(op, m, dobs, w)
+        x = torch.tensor(m, device=cuda, requires_grad=True)
+        phi = eng.misfit(x, torch.tensor(dobs, device=cuda), torch.tensor(w, device=cuda))
+        phi.backward()
+        with torch.no_grad():
+            d = eng.dpred(torch.tensor(m, device=cuda))
+        eng.check()
+        td, tg = TOL[dtype]
+        assert rel(d, d_ref) < td
+        assert rel(x.grad, g_ref) < tg

@@ -103,7 +103,7 @@ def test_refined_octree_half_space_potential():
     assert np.abs(v / ana - 1).max() < 0.05, v / ana
 
 
-def test_config5_builder_shapes():
+def test_refined_3d_workload_builder_shapes():
     tm, sv, m = syn.dc3d_tree(seed=0, max_level=6, n_el=7, n_sources=12, n_rx=5,
                               refine=((6, 10.0), (5, 30.0), (4, 60.0)))
     assert m.size == tm.nC and np.all(np.isfinite(m))
