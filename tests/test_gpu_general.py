@@ -132,3 +132,27 @@ def test_general_rejects_unsymmetric_patterns_and_other_dtypes(cuda):
     with pytest.raises(NotImplementedError):
         make_solver(torch.tensor(c2), torch.tensor(k2), n2, 1, device=cuda,
                     dtype=torch.float32, matrix_type="general")
+
+
+def test_general_static_pivoting_and_nonfinite_pivots(cuda):
+    """A zero diagonal (every pivot of the first elimination step zero) is
+    replaced by the static bound and counted, with finite results; a NaN
+    value records a zero-pivot error that check() raises."""
+    crow, col, n, vals = _general_systems("2d", 1, 8)
+    r = O.row_of(crow)
+    v = vals[0].copy()
+    v[r == col] = 0.0
+    s = make_solver(torch.tensor(crow), torch.tensor(col), n, 1, device=cuda,
+                    matrix_type="general")
+    s.factorize(torch.tensor(v, device=cuda))
+    x = s.solve(torch.tensor(np.ones(n), device=cuda))
+    s.check()
+    assert s.static_pivots() > 0
+    assert torch.isfinite(x).all()
+    v2 = vals[0].copy()
+    v2[0] = np.nan
+    s.factorize(torch.tensor(v2, device=cuda))
+    s.solve(torch.tensor(np.ones(n), device=cuda))
+    with pytest.raises(nat.DCTError):
+        s.check()
+    s.free()
