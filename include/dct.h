@@ -349,7 +349,7 @@ int dct_plan_create_general(const dct_symbolic* sym, int32_t nbatch, int32_t max
 int dct_solve_transposed(dct_plan* plan, const void* d_b, int32_t io_dtype,
                          int32_t b_batched, int32_t k, void* d_x, void* stream);
 /* Number of pivots static pivoting replaced in the last factorization of a
- * general plan (synchronises the stream). */
+ * general plan (synchronises the stream; dct_check_status leaves it). */
 int dct_plan_static_pivots(dct_plan* plan, void* stream, int32_t* count);
 
 /* ---- self-test of the bounded device waits ---------------------------------

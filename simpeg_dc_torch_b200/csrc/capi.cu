@@ -1187,7 +1187,9 @@ int dct_check_status(dct_plan* P, void* stream, int32_t* code, int32_t* where,
   DCT_CUDA(cudaMemcpyAsync(rb, P->resid_bits, sizeof(rb), cudaMemcpyDeviceToHost, st),
            "status read");
   DCT_CUDA(cudaStreamSynchronize(st), "stream synchronize");
-  DCT_CUDA(cudaMemsetAsync(P->status, 0, 64, st), "status reset");
+  // the error words; the static-pivot count (status[4]) lives until the
+  // next factorization
+  DCT_CUDA(cudaMemsetAsync(P->status, 0, 4 * sizeof(int), st), "status reset");
   if (code) *code = hs[0];
   if (where) *where = hs[0] ? hs[1] : -1;
   if (residual) {
