@@ -1,9 +1,10 @@
 """The side engines at the large 2.5-D configuration (56,525 nodes, 10
 wavenumbers, 186 sources) against the CPU oracle: the linearized IP engine
 (dctorch/ip2d.py: data J(m_dc) eta and the misfit gradient in eta, with every
-other receiver of apparent-chargeability type) and the joint non-linear
-DC + IP engine (dctorch/dcip2d.py: both data kinds and the gradient in
-(log-rho, logit-eta)).  The oracle solves exactly with the block-tridiagonal
+other receiver of apparent-chargeability type), its 3-D counterpart
+(dctorch/ip3d.py) on a 75,843-node grid with 200 sources, and the joint
+non-linear DC + IP engine (dctorch/dcip2d.py: both data kinds and the
+gradient in (log-rho, logit-eta)).  The oracle solves exactly with the block-tridiagonal
 slab Cholesky.  float64 is held to 1e-10 (data) / 1e-9 (gradients);
 float32 + refinement to 1e-6 / 1e-5, the levels of the DC scale tests."""
 import numpy as np
@@ -11,7 +12,7 @@ import pytest
 import torch
 
 from oracle import dc_oracle as O
-from simpeg_dc_torch_b200 import TorchDCIP2D, TorchIP2D
+from simpeg_dc_torch_b200 import TorchDCIP2D, TorchIP2D, TorchIP3D
 from simpeg_dc_torch_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -97,3 +98,30 @@ def test_dcip2d_large_against_oracle(cuda):
     assert rel(a, d_dc) < 1e-10 and rel(b, d_ip) < 1e-10
     assert abs(float(phi.detach()) - phi_ref) <= 1e-9 * phi_ref
     assert rel(x.grad, g_ref) < 1e-9
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_ip3d_mid_against_oracle(cuda, dtype):
+    mesh, survey, m = syn.dc3d(seed=0, ncore=(40, 40, 20), dx=8.0, npad=6)
+    flags = _mark_every_other(survey)
+    ip = TorchIP3D(mesh, survey, m, device=cuda, dtype=dtype)
+    ops = ip.dc._ops
+    op = dict(L3=ip.dc._L, crow=ops.crow, col=ops.col, nN=ops.nN, Q=ops.q.toarray(),
+              Pd=ops.Pd, sidx=ops.sidx, slab=O.grid_slabs(mesh.node_grid_index()))
+    charge = np.repeat(flags, [rx.nD for s in survey.source_list for rx in s.receiver_list])
+    eta = np.random.default_rng(11).uniform(0.0, 0.2, ip.dc.nC)
+    v_dc = O.dpred_3d(op, m)
+    scale = O.ip_scale(v_dc, charge)
+    d_ref = scale * O.jvec_3d(op, m, eta)
+    dobs = d_ref * 1.05
+    w = 1.0 / (np.abs(dobs) + 1e-3 * np.abs(dobs).max())
+    g_ref = O.jtvec_3d(op, m, scale * 2.0 * w * w * (d_ref - dobs))
+    et = torch.tensor(eta, device=cuda, requires_grad=True)
+    phi = ip.misfit(et, torch.tensor(dobs, device=cuda), torch.tensor(w, device=cuda))
+    phi.backward()
+    with torch.no_grad():
+        d = ip.dpred(et)
+    ip.check()
+    td, tg = TOL[dtype]
+    assert rel(d, d_ref) < td
+    assert rel(et.grad, g_ref) < tg
