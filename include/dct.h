@@ -319,8 +319,8 @@ int dct_values_vjp_multi(int64_t nC, int32_t nb, const int64_t* d_Lt_ptr,
  * right-hand sides, b and x row-major (n, k) float64 on the current device.
  * Its only scratch is a fixed 2 MiB array in the library (held by every GPU
  * that loads the library until exit); sizes beyond the limits return
- * DCT_ERR_ARG.  The first call on a device looks up that array's address and
- * should come before any stream capture.  Calls share the array, so calls
+ * DCT_ERR_ARG.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) and caches it.  Calls share the array, so calls
  * that may overlap on the GPU race and must be ordered.  The call does not
  * wait for the GPU: a matrix that is not positive definite (a non-positive
  * or NaN pivot) makes every entry of x NaN rather than returning a status.

@@ -13,11 +13,10 @@
 // In host code `g_noalloc_factor` is a host-side stand-in, not a device
 // address; its device address is obtained once per device with
 // cudaGetSymbolAddress (with that device current) on the first call made on
-// that device, and cached.  That first call should therefore come before any
-// stream capture.  All calls share the one array and it keeps the contents of
-// the last call: each call clears the part it uses before writing it, and two
-// calls whose work overlaps on the GPU (different streams, no ordering) race
-// on it and must not be issued.
+// that device, and cached.  All calls share the one array and it keeps the
+// contents of the last call: each call clears the part it uses before writing
+// it, and two calls whose work overlaps on the GPU (different streams, no
+// ordering) race on it and must not be issued.
 //
 // The call returns without waiting for the GPU, so it cannot return a status
 // for a matrix that is not positive definite: a non-positive or NaN pivot
