@@ -831,7 +831,7 @@ int dct_plan_create_tuned(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs
       const int ns = S.ns(s), N = S.front_n[s];
       for (int q = 0; q * dct::kPanel < ns; ++q) {
         img_off.push_back(acc);
-        if (N > small_max) acc += int64_t(4) * dct::img_groups(q, ns, N) * 256;
+        if (N > small_max) acc += dct::img_floats(dct::img_groups(q, ns, N));
       }
     }
     pan_first[S.nsuper] = int32_t(img_off.size());

@@ -127,9 +127,16 @@ __host__ __device__ inline UpdateRange update_range(int p, int ns, int N, int bp
 // groups of zero padding so that any 128-row window that starts below the
 // front's last row lies inside it.  Each element is stored twice, hi =
 // tf32(x) and lo = x - hi, in the tensor cores' K-major layout without
-// swizzle: [hl][K stage of 32 columns][8-row group][K core of 4][row of 8]
-// [column of 4] floats, so 128 rows x 32 columns of one of hi/lo are 16 KB
-// contiguous (core matrices 128 B apart along K, 8-row groups 1 KB apart).
+// swizzle: [hl][K stage of kImgK columns][8-row group][K core of 4][row of 8]
+// [column of 4] floats, so 128 rows x kImgK columns of one of hi/lo are
+// 128 * kImgK * 4 bytes contiguous (16 KB for 32 columns; core matrices
+// 128 B apart along K, 8-row groups 32 * kImgK bytes apart).  The stage
+// width is the K depth of one bulk copy of the trailing update.
+#ifndef DCT_IMG_K
+#define DCT_IMG_K 32
+#endif
+constexpr int kImgK = DCT_IMG_K;
+static_assert(kImgK % 8 == 0 && kPanel % kImgK == 0, "image stages: 8 .. 64 columns");
 __host__ __device__ inline int img_origin(int q, int ns) {
   const int c0 = q * kPanel;
   const int w = ns - c0 < kPanel ? ns - c0 : kPanel;
@@ -141,8 +148,11 @@ __host__ __device__ inline int img_groups(int q, int ns, int N) {
 // float offset of (hl, K stage, group g, column k of the stage, row r8 of the
 // group) in a panel image of G groups
 __host__ __device__ inline int64_t img_index(int G, int hl, int stage, int g, int k, int r8) {
-  return (int64_t(hl * 2 + stage) * G + g) * 256 + (k >> 2) * 32 + r8 * 4 + (k & 3);
+  return (int64_t(hl * (kPanel / kImgK) + stage) * G + g) * (8 * kImgK) + (k >> 2) * 32 +
+         r8 * 4 + (k & 3);
 }
+// floats of one panel image of G groups (hi and lo, all stages)
+__host__ __device__ inline int64_t img_floats(int G) { return int64_t(2) * kPanel * 8 * G; }
 struct ImgArgs {
   float* img;                // nbatch * stride floats
   const int64_t* off;        // per panel (pan_first[s] + q): first float

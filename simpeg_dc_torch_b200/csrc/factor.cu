@@ -296,8 +296,8 @@ k_large_panel(DevSym S, const PanelTask* __restrict__ tasks, T* fronts,
           const int gr = r0 + r - R0;
           const float v = float(acc[p][q]);
           const uint32_t h = tf32_rna(v);
-          img[img_index(G, 0, c >> 5, gr >> 3, c & 31, gr & 7)] = __uint_as_float(h);
-          img[img_index(G, 1, c >> 5, gr >> 3, c & 31, gr & 7)] = v - __uint_as_float(h);
+          img[img_index(G, 0, c / kImgK, gr >> 3, c % kImgK, gr & 7)] = __uint_as_float(h);
+          img[img_index(G, 1, c / kImgK, gr >> 3, c % kImgK, gr & 7)] = v - __uint_as_float(h);
         }
       }
     }

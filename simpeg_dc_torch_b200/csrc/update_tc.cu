@@ -5,10 +5,15 @@
 //
 // One CTA per output tile, warp-specialised:
 //   warp 0    one thread issues the bulk copies (cp.async.bulk ... complete_tx)
-//             of each K stage -- 32 columns of the hi and lo images of the
-//             tile's row block i and column block j, 16 KB each, contiguous in
-//             the images -- into a two-stage ring, each stage guarded by a
-//             "full" mbarrier (transaction bytes) and an "empty" one;
+//             of each K stage -- kImgK columns of the hi and lo images of the
+//             tile's row block i and column block j, 16 KB each for 32
+//             columns, contiguous in the images -- into a ring of stages that
+//             fills kURingBytes (two stages of 64 KB), each stage guarded by
+//             a "full" mbarrier (transaction bytes) and an "empty" one.
+//             Deeper rings of smaller stages (16 columns: four or five stages
+//             of 32 KB) measured slower on the 269,001-node benchmark (+1.5 %
+//             / +6 % on this kernel): the copies' latency is not what bounds
+//             it, the per-tile prologue and epilogue of one CTA per SM are;
 //   warp 1    allocates TMEM and one thread issues tcgen05.mma kind::tf32 for
 //             each stage (3xTF32: hi*hi + hi*lo + lo*hi; Markidis et al. 2018,
 //             Ootomo & Yokota 2022), then commits to the stage's "empty"
@@ -39,17 +44,24 @@
 namespace dct {
 namespace {
 
+#ifndef DCT_U_RING_KB
+#define DCT_U_RING_KB 160
+#endif
 constexpr int kUThreads = 192;
-constexpr int kUStages = 2;
-constexpr int kUChunk = 16384;              // 128 rows x 32 columns, hi or lo
+constexpr int kUChunk = 128 * kImgK * 4;    // 128 rows x kImgK columns, hi or lo
 constexpr int kUStageBytes = 4 * kUChunk;   // A hi, A lo, B hi, B lo
-constexpr uint32_t kULbo = 128, kUSbo = 1024;
+constexpr int kURingBytes = DCT_U_RING_KB * 1024;
+constexpr int kUStages = kURingBytes / kUStageBytes;
+constexpr uint32_t kULbo = 128, kUSbo = 32 * kImgK;
+static_assert(kUStages >= 2, "at least two stages in the copy ring");
 constexpr int kUAcc = 4;                    // accumulators: one per panel
 constexpr int kUTileBytes = kTcM * kTcN * 4;   // the output tile, staged
 constexpr size_t kUSmem = size_t(kUStages) * kUStageBytes + kUTileBytes + 128;
 static_assert(kUAcc * 128 <= 512, "TMEM columns of one SM");
 static_assert(size_t(kUStages) * kUStageBytes >= sizeof(float) * kDiagSmemElems,
               "the ring also holds factor_diag's workspace");
+static_assert(kUSmem <= 227 * 1024, "shared memory of one CTA");
+static_assert(2 * kUStages * 8 + 8 + 4 <= 128, "barriers and the TMEM slot");
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
@@ -117,7 +129,7 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   const bool diag = tk.t0 == tk.t1;
   const int jn = min(kTcN, R.cend - rj);    // tile columns that can be written
   const int np = (jn + 15) & ~15;           // MMA N: a multiple of 16
-  const int nst = (base - R.ka + 31) / 32;
+  const int nst = (base - R.ka + kImgK - 1) / kImgK;
   const int nacc = (base - R.ka + kPanel - 1) / kPanel;
 
   if (warp == 1) tmem_alloc(tmem_slot, kUAcc * 128);
@@ -136,11 +148,11 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
   const int pan0 = im.pan_first[s];
   // the 16 KB chunk of rows row0 .. row0 + 127, K stage st, hi (0) / lo (1)
   auto chunk = [&](int row0, int st, int hl) -> const float* {
-    const int kcol = R.ka + 32 * st;
+    const int kcol = R.ka + kImgK * st;
     const int q = kcol / kPanel;
     const int G = img_groups(q, ns, N);
     const int g0 = (row0 - img_origin(q, ns)) >> 3;
-    return img + im.off[pan0 + q] + img_index(G, hl, (kcol % kPanel) / 32, g0, 0, 0);
+    return img + im.off[pan0 + q] + img_index(G, hl, (kcol % kPanel) / kImgK, g0, 0, 0);
   };
 
   bool ok = true;
@@ -183,10 +195,10 @@ k_update_tc(DevSym S, const PanelTask* __restrict__ tasks, float* fronts,
         const uint32_t al = ah + kUChunk;
         const uint32_t bh = diag ? ah : ah + 2 * kUChunk;
         const uint32_t bl = diag ? al : ah + 3 * kUChunk;
-        const int kcol = R.ka + 32 * st;
+        const int kcol = R.ka + kImgK * st;
         const uint32_t acc = tmem + uint32_t(((kcol - R.ka) / kPanel) * 128);
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
+        for (int kk = 0; kk < kImgK / 8; ++kk) {
           const uint32_t ko = uint32_t(kk) * 2 * kULbo;
           const uint64_t dah = umma_desc(ah + ko, kULbo, kUSbo);
           const uint64_t dal = umma_desc(al + ko, kULbo, kUSbo);

@@ -15,6 +15,7 @@ import numpy as np
 PANEL = 64
 UTILE = 64
 TCTILE = 128
+IMG_K = 32           # columns of one K stage of the panel images (DCT_IMG_K)
 (SMALL, LSCATTER, LEXTEND, LPANEL, LUPDATE, PINV, LINVINIT, LINVT, LINVX,
  FWDSMALL, FWDLINV, FWDBND, BWDSMALL, BWDGEMM, BWDLINV, FWDLINVTC, FWDBNDTC,
  BWDGEMMTC, BWDLINVTC) = range(19)
@@ -73,7 +74,8 @@ def img_groups(q, ns, N):
 
 
 def img_index(G, hl, stage, g, k, r8):
-    return ((hl * 2 + stage) * G + g) * 256 + (k >> 2) * 32 + r8 * 4 + (k & 3)
+    return (((hl * (PANEL // IMG_K) + stage) * G + g) * (8 * IMG_K) + (k >> 2) * 32 + r8 * 4
+            + (k & 3))
 
 
 def image_offsets(S):
@@ -85,31 +87,32 @@ def image_offsets(S):
         for q in range(-(-ns // PANEL)):
             off[(s, q)] = acc
             if N > SMALL_F32:
-                acc += 4 * img_groups(q, ns, N) * 256
+                acc += 2 * PANEL * 8 * img_groups(q, ns, N)
     return off, acc
 
 
-# element (m, k) of a 128-row x 32-column image chunk
-_CHUNK_M, _CHUNK_K = np.meshgrid(np.arange(128), np.arange(32), indexing="ij")
-_CHUNK_IDX = ((_CHUNK_M // 8) * 256 + (_CHUNK_K // 4) * 32 + (_CHUNK_M % 8) * 4
+# element (m, k) of a 128-row x IMG_K-column image chunk
+_CHUNK_M, _CHUNK_K = np.meshgrid(np.arange(128), np.arange(IMG_K), indexing="ij")
+_CHUNK_IDX = ((_CHUNK_M // 8) * (8 * IMG_K) + (_CHUNK_K // 4) * 32 + (_CHUNK_M % 8) * 4
               + _CHUNK_K % 4)
 
 
 def _image_operand(dinv, s, ns, N, row0, ka, nst):
-    """The (128, 32 nst) operand the tensor-core update streams from the
-    panel images for tile rows row0 .. row0 + 127 and K stages of 32 columns
+    """The (128, IMG_K nst) operand the tensor-core update streams from the
+    panel images for tile rows row0 .. row0 + 127 and K stages of IMG_K columns
     from ka, with every chunk bounds-checked against its panel's image."""
     img = dinv[("img", 0)]
     parts = []
     for st in range(nst):
-        kcol = ka + 32 * st
-        q, h = kcol // PANEL, (kcol % PANEL) // 32
+        kcol = ka + IMG_K * st
+        q, h = kcol // PANEL, (kcol % PANEL) // IMG_K
         G, R0q = img_groups(q, ns, N), img_origin(q, ns)
         assert row0 >= R0q and (row0 - R0q) % 8 == 0
         off = dinv[("imgoff", s, q)]
         lo = off + img_index(G, 0, h, 0, 0, 0)
         start = off + img_index(G, 0, h, (row0 - R0q) // 8, 0, 0)
-        assert lo <= start and start + 4096 <= lo + G * 256, "chunk outside its image"
+        assert lo <= start and start + 128 * IMG_K <= lo + G * 8 * IMG_K, \
+            "chunk outside its image"
         parts.append(img[start + _CHUNK_IDX])
     return np.hstack(parts)
 
@@ -185,8 +188,8 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE, bpan=1):
             rr, cc = np.meshgrid(np.arange(nr), np.arange(w), indexing="ij")
             gr = r0 + rr - R0q
             assert gr.min() >= 0 and gr.max() < 8 * (G - 16)
-            idx = off + img_index(G, 0, cc >> 5, gr >> 3, cc & 31, gr & 7)
-            assert idx.max() < off + 2 * G * 256
+            idx = off + img_index(G, 0, cc // IMG_K, gr >> 3, cc % IMG_K, gr & 7)
+            assert idx.max() < off + PANEL * 8 * G
             img[idx] = F[r0:r0 + nr, c0:c0 + w]
     elif kind == LUPDATE:
         c0 = p * PANEL
@@ -210,7 +213,7 @@ def _task_factor(S, kind, tk, fronts, vals, arg, dinv, utile=UTILE, bpan=1):
         if utile == TCTILE:
             # the tensor-core kernel's operands come from the panel images:
             # they must hold exactly these rows of L
-            nst = (base - ka + 31) // 32
+            nst = (base - ka + IMG_K - 1) // IMG_K
             Ai = _image_operand(dinv, s, ns, N, R0 + t0 * utile, ka, nst)
             Bj = _image_operand(dinv, s, ns, N, R0 + t1 * utile, ka, nst)
             full = Ai @ Bj.T
