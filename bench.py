@@ -450,6 +450,31 @@ def cpu_baseline_leg(name):
                     "restatement of the reference's CPU path"}
 
 
+def factor_once(args, mesh, survey, m_np, dev):
+    """One float32 factorization inside the NVTX range `fact_once`, after a
+    warm eval+grad and a warm factorization: the launch list of one
+    factorization for ncu (--nvtx --nvtx-include "fact_once/")."""
+    import torch
+    e32 = make_engine(args.workload, mesh, survey, dev, torch.float32)
+    m = torch.tensor(m_np, device=dev, requires_grad=True)
+    with torch.no_grad():
+        d = e32.dpred(m)
+    e32.misfit(m, d * 1.05, 1.0 / d.abs()).backward()
+    _, vals = e32._path.values(m.detach())
+    e32._path.factorize(vals)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("fact_once")
+    a.record()
+    e32._path.factorize(vals)
+    b.record()
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    e32.check()
+    print(json.dumps({"workload": args.workload, "factorization_ms": a.elapsed_time(b)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -463,6 +488,10 @@ def main():
     ap.add_argument("--side", action="store_true",
                     help="also time the complex-resistivity and DC-IP engines "
                          "(2.5-D workloads)")
+    ap.add_argument("--factor-once", action="store_true",
+                    help="profiling mode: one float32 eval+grad, then one "
+                         "factorization inside the NVTX range fact_once (3-D "
+                         "workloads); prints its time and no bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -490,6 +519,8 @@ def main():
         return max_over_ranks(x, world, dev)
 
     mesh, survey, m_np = build_case(args.workload, seed=rank)
+    if args.factor_once:
+        return factor_once(args, mesh, survey, m_np, dev)
     e32 = make_engine(args.workload, mesh, survey, dev, torch.float32)
     e64 = make_engine(args.workload, mesh, survey, dev, torch.float64)
     m = torch.tensor(m_np, device=dev)

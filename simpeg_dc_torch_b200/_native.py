@@ -13,7 +13,9 @@ import threading
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libdct.so")
+# DCT_LIB_PATH selects another build of the same sources (for example one
+# compiled with different -D knobs, to compare kernels); unset: the in-tree build
+LIB_PATH = os.environ.get("DCT_LIB_PATH") or os.path.join(_HERE, "lib", "libdct.so")
 
 F64, F32, C128 = 0, 1, 2
 

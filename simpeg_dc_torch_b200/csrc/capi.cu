@@ -530,6 +530,35 @@ void build_inverse_schedule(const dct::Symbolic& S, int small_max,
   inv->launches.push_back({dct::kPanelInverse, 0, 0, int64_t(inv->tasks.size()), 0});
 }
 
+// Float32 plans of one system: the trailing-update launches with many tiles
+// and few fronts run persistent CTAs (update_tc.cu), which need the diagonal
+// tile of every front -- the one whose CTA then factors the next diagonal
+// block -- ahead of the other tiles.  The tiles of one launch are
+// independent, so the order inside a launch is free.
+#ifndef DCT_U_PERSISTENT
+#define DCT_U_PERSISTENT 1
+#endif
+#ifndef DCT_U_PERSIST_MAX_FRONTS
+#define DCT_U_PERSIST_MAX_FRONTS 32
+#endif
+void plan_persistent_updates(dct_plan* P) {
+  P->update_nspec.assign(P->fact.launches.size(), -1);
+  if (!DCT_U_PERSISTENT || P->dtype != DCT_F32 || P->nbatch != 1) return;
+  auto diagonal = [](const PanelTask& t) { return t.t0 < 0 || (t.t0 == 0 && t.t1 == 0); };
+  for (size_t li = 0; li < P->fact.launches.size(); ++li) {
+    const Launch& L = P->fact.launches[li];
+    if (L.kind != dct::kLargeUpdate || L.count <= 0) continue;
+    auto b = P->fact.tasks.begin() + L.first;
+    auto e = b + L.count;
+    const int64_t nspec = std::count_if(b, e, diagonal);
+    const int64_t pers = int64_t(P->sm_count) - nspec;
+    // each persistent CTA takes two tiles or more
+    if (nspec > DCT_U_PERSIST_MAX_FRONTS || pers < 1 || L.count - nspec < 2 * pers) continue;
+    std::stable_partition(b, e, diagonal);
+    P->update_nspec[li] = static_cast<int32_t>(nspec);
+  }
+}
+
 int upload_schedule(dct_plan* P, dct::Schedule* sch) {
   const PanelTask* d = nullptr;
   int rc = upload(P, sch->tasks, &d);
@@ -806,6 +835,13 @@ int dct_plan_create_tuned(const dct_symbolic* h, int32_t nbatch, int32_t max_rhs
   build_factor_schedule(S, small_max, update_tile(dtype), P->tune.update_block,
                         dtype == DCT_F32, &P->fact);
   P->update_bpan = P->tune.update_block;
+  {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+        sms > 0)
+      P->sm_count = sms;
+  }
+  plan_persistent_updates(P);
   build_solve_schedules(S, dtype, P->tune, &P->fwd, &P->bwd);
   std::vector<int64_t> dinv_off;
   build_inverse_schedule(S, small_max, &P->inv, &dinv_off, &P->dinv_stride);

@@ -261,6 +261,11 @@ struct dct_plan {
   double ir_tol = 0.0;             // stop once the estimated error is below (0: fixed count)
   dct::IrState* ir = nullptr;      // device: refinement state of the last solve
   int update_bpan = 1;             // panels per trailing-update block
+  int sm_count = 148;              // multiprocessors of the plan's device
+  // per factor launch: for float32 trailing updates that run persistent CTAs,
+  // the number of diagonal tasks moved to the front of the launch's tasks
+  // (one CTA each); -1: one CTA per task
+  std::vector<int32_t> update_nspec;
   dct::Profiler prof;
   // general (unsymmetric-valued) float64 plans, factored P A P^T = L U with
   // static pivoting: `fronts` holds L (unit diagonal) in the lower part,
@@ -304,8 +309,10 @@ struct SolveArgs {
 // one launch of a tensor-core substitution kind (kFwdLinvTc .. kBwdLinvTc)
 cudaError_t launch_solve_tc(int kind, const SolveArgs<float>& g, int64_t count,
                             int nbatch, cudaStream_t st);
-// one launch of the float32 trailing update (update_tc.cu)
-cudaError_t launch_update_tc(dct_plan* P, const PanelTask* tasks, int64_t count,
+// one launch of the float32 trailing update (update_tc.cu); nspec >= 0:
+// the first nspec tasks take one CTA each and persistent CTAs on the
+// remaining multiprocessors share the others, nspec = -1: one CTA per task
+cudaError_t launch_update_tc(dct_plan* P, const PanelTask* tasks, int64_t count, int nspec,
                              cudaStream_t st);
 // records the message returned by dct_last_error() for this thread
 void set_last_error(const char* msg);

@@ -691,7 +691,8 @@ cudaError_t factor_impl(dct_plan* P, const void* vals, int vals_dtype,
         break;
       case kLargeUpdate:
         if constexpr (sizeof(T) == 4) {
-          e = launch_update_tc(P, t, L.count, st);
+          e = launch_update_tc(
+              P, t, L.count, li < P->update_nspec.size() ? P->update_nspec[li] : -1, st);
         } else {
           e = launch_pdl(k_large_update<T>, grid, dim3(kThreads), update_smem, st, P->ds, t,
                          fronts, P->front_stride, static_cast<T*>(P->dinv), P->d_dinv_off,
