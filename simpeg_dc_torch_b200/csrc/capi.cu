@@ -265,6 +265,11 @@ void account_solve(const dct::Symbolic& S, dct::Schedule* sc, double es) {
 // (tcgen05 tensor-core tiles, M = N = 128)
 int update_tile(int dtype) { return dtype == DCT_F32 ? 128 : dct::kUpdateTile; }
 
+#ifndef DCT_SMALL_BUCKETS
+#define DCT_SMALL_BUCKETS 1
+#endif
+constexpr int kSmallBucketMin = 256;   // fronts: about two CTAs per SM of a B200
+
 void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int bpan,
                            bool align8, dct::Schedule* out) {
   auto& T = out->tasks;
@@ -276,12 +281,35 @@ void build_factor_schedule(const dct::Symbolic& S, int small_max, int utile, int
       (S.front_n[s] <= small_max ? small : large).push_back(s);
     }
     if (!small.empty()) {
-      Launch l{dct::kSmallFront, lv, int64_t(T.size()), int64_t(small.size()), 0};
-      for (int s : small) {
-        T.push_back({s, 0, 0, 0});
-        l.arg = std::max(l.arg, S.front_n[s]);
+      // The single-CTA kernel's shared memory is set by the largest front of
+      // its launch, so the level's small fronts go into launches by order
+      // (bounds at multiples of 32 rows): the smaller fronts then fit more
+      // CTAs per SM.  A launch of fewer than kSmallBucketMin fronts would
+      // leave most SMs idle and joins the next larger bucket.
+      std::stable_sort(small.begin(), small.end(),
+                       [&](int a, int b) { return S.front_n[a] < S.front_n[b]; });
+      size_t i0 = 0;
+      while (i0 < small.size()) {
+        size_t i1 = small.size();
+        if (DCT_SMALL_BUCKETS) {
+          int bound = (S.front_n[small[i0]] + 31) / 32 * 32;
+          for (;;) {
+            i1 = i0;
+            while (i1 < small.size() && S.front_n[small[i1]] <= bound) ++i1;
+            if (i1 == small.size() || i1 - i0 >= size_t(kSmallBucketMin)) break;
+            bound += 32;
+          }
+          // a last bucket too small to stand alone joins this one
+          if (small.size() - i1 < size_t(kSmallBucketMin)) i1 = small.size();
+        }
+        Launch l{dct::kSmallFront, lv, int64_t(T.size()), int64_t(i1 - i0), 0};
+        for (size_t i = i0; i < i1; ++i) {
+          T.push_back({small[i], 0, 0, 0});
+          l.arg = std::max(l.arg, S.front_n[small[i]]);
+        }
+        L.push_back(l);
+        i0 = i1;
       }
-      L.push_back(l);
     }
     if (large.empty()) continue;
     {
