@@ -123,6 +123,54 @@ __global__ void k_gather_contract(int nbatch, int64_t n, int64_t nnz, int k,
   }
 }
 
+// The same contraction (permuted Y and X, k <= 32 R) with one warp per run
+// of kGcRun consecutive entries: the row of Y stays in registers while
+// consecutive entries share it, as they do in CSR order (about 27 entries
+// per row on a 3-D grid), so Y is read about once per row instead of once per
+// entry.  Any entry order gives the same result.
+#ifndef DCT_GC_ROWS
+#define DCT_GC_ROWS 1
+#endif
+constexpr int kGcRun = 32;
+template <int R>
+__global__ void k_gather_contract_rows(int nbatch, int64_t n, int64_t nnz, int k,
+                                       const int32_t* __restrict__ row,
+                                       const int32_t* __restrict__ col,
+                                       const int32_t* __restrict__ iperm,
+                                       const double* __restrict__ scale,
+                                       const double* __restrict__ Y,
+                                       const double* __restrict__ X, double* __restrict__ gv) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  const int64_t runs = (nnz + kGcRun - 1) / kGcRun;
+  const int64_t total = runs * nbatch;
+  for (int64_t t = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; t < total;
+       t += warps) {
+    const int b = static_cast<int>(t / runs);
+    const int64_t e0 = (t - int64_t(b) * runs) * kGcRun;
+    const int64_t e1 = e0 + kGcRun < nnz ? e0 + kGcRun : nnz;
+    const double sc = -(scale != nullptr ? scale[b] : 1.0);
+    int64_t cur = -1;
+    double y[R];
+    for (int64_t e = e0; e < e1; ++e) {
+      const int64_t r = iperm[row[e]];
+      if (r != cur) {
+        cur = r;
+        const double* yr = Y + (int64_t(b) * n + r) * k;
+#pragma unroll
+        for (int q = 0; q < R; ++q) y[q] = lane + 32 * q < k ? yr[lane + 32 * q] : 0.0;
+      }
+      const double* x = X + (int64_t(b) * n + iperm[col[e]]) * k;
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        if (lane + 32 * q < k) acc += y[q] * x[lane + 32 * q];
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) gv[int64_t(b) * nnz + e] = sc * acc;
+    }
+  }
+}
+
 // complex128: gv[b, e] = -sum_r Y[b, row_e, r] X[b, col_e, r] (no
 // conjugation: the caller conjugates where its convention asks)
 __global__ void k_gather_contract_c(int nbatch, int64_t n, int64_t nnz, int k,
@@ -222,8 +270,22 @@ int dct_gather_contract(int32_t nbatch, int64_t n, int64_t nnz, int32_t k,
     return DCT_ERR_ARG;
   if (nnz == 0) return DCT_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_gather_contract<double, true><<<blocks_for(nnz * nbatch * 32, kT), kT, 0, st>>>(
-      nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
+  const int64_t run_threads = (nnz + kGcRun - 1) / kGcRun * nbatch * 32;
+  if (!DCT_GC_ROWS)
+    k_gather_contract<double, true><<<blocks_for(nnz * nbatch * 32, kT), kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
+  else if (k <= 64)
+    k_gather_contract_rows<2><<<blocks_for(run_threads, kT), kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
+  else if (k <= 128)
+    k_gather_contract_rows<4><<<blocks_for(run_threads, kT), kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
+  else if (k <= 256)
+    k_gather_contract_rows<8><<<blocks_for(run_threads, kT), kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
+  else
+    k_gather_contract<double, true><<<blocks_for(nnz * nbatch * 32, kT), kT, 0, st>>>(
+        nbatch, n, nnz, k, d_row, d_col, d_iperm, d_scale, d_Y, d_X, d_gv);
   return report(cudaGetLastError());
 }
 
