@@ -26,3 +26,19 @@ def test_reference_arm_prints_one_contract_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("port", "reference")
     assert d["config"]["workload"] == "dc2d_small"
+
+
+def test_library_path_override():
+    """DCT_LIB_PATH selects another build of the same sources (A/B timing);
+    unset, the in-tree library is the one loaded."""
+    code = "from simpeg_dc_torch_b200 import _native as n; print(n.LIB_PATH)"
+    env = dict(os.environ)
+    env.pop("DCT_LIB_PATH", None)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=300, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == os.path.join(ROOT, "simpeg_dc_torch_b200", "lib", "libdct.so")
+    env["DCT_LIB_PATH"] = "/tmp/other/libdct.so"
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=300, cwd=ROOT, env=env)
+    assert r.returncode == 0 and r.stdout.strip() == "/tmp/other/libdct.so"
