@@ -9,10 +9,12 @@ Pinned: `tests/golden/*.npz` hold outputs of the reference itself (its
 runtime, driven with the same operators); `tests/test_oracle.py` checks this
 module against them.
 
-Two exact float64 solvers stand behind it: `SuperLUBatch` (the reference's
-own CPU solver, scipy SuperLU) and `SlabCholeskyBatch`, a block-tridiagonal
-dense Cholesky over the grid slabs for the workloads at which SuperLU takes
-minutes per factorization (selected by an operator set's "slab" entry).
+Three exact solvers stand behind it: `SuperLUBatch` (the reference's own
+CPU solver, scipy SuperLU, real or complex), `SlabCholeskyBatch`, a
+block-tridiagonal dense Cholesky over the grid slabs for the float64
+workloads at which SuperLU takes minutes per factorization (selected by an
+operator set's "slab" entry), and `SlabLUBatch`, the same slabs factored by
+block LU for complex-symmetric (complex resistivity) and general systems.
 
 Operators (names as in the reference engines):
   Lstack  : CSR (nky*nnzA, nC), values of A_k = rows k*nnzA .. (k+1)*nnzA
